@@ -1,0 +1,157 @@
+/*
+ * vsfeel_bm3d.h -- C ABI of the B200-native BM3Dv2 basic estimate.
+ *
+ * The entry points mirror the VapourSynth filter that the reference
+ * registers as core.vsfeel.BM3Dv2 (src/bm3d.cpp:1558-1574):
+ *
+ *   vsfeel_bm3d_create      <- BM3DCreate      src/bm3d.cpp:1043-1552
+ *   vsfeel_bm3d_frame_range <- BM3DGetFrame, arInitial         :704-712
+ *   vsfeel_bm3d_get_frame   <- BM3DGetFrame, arAllFramesReady  :713-1025
+ *   vsfeel_bm3d_free        <- BM3DFree                        :1030-1037
+ *
+ * plus clip-level entry points (host or device buffers) that a batch caller
+ * or the torch extension uses instead of per-frame callbacks.
+ *
+ * Conventions: pure C, no exceptions cross the boundary. Every function
+ * returns 0 on success or a negative VSFEEL_E_* code; the message (prefixed
+ * "BM3D: " like the reference's errors) is available from
+ * vsfeel_bm3d_last_error() on the calling thread. A context is internally
+ * synchronised: calls from several threads are serialised. Strides are in
+ * bytes for host buffers and in elements (floats) for device buffers.
+ */
+#ifndef VSFEEL_BM3D_H
+#define VSFEEL_BM3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VSFEEL_BM3D_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define VSFEEL_API __attribute__((visibility("default")))
+#else
+#define VSFEEL_API
+#endif
+
+enum {
+    VSFEEL_OK = 0,
+    VSFEEL_E_ARG = -1,      /* invalid argument (message names it)          */
+    VSFEEL_E_FORMAT = -2,   /* unsupported clip format                      */
+    VSFEEL_E_CUDA = -3,     /* CUDA runtime error                           */
+    VSFEEL_E_MEMORY = -4,   /* device or pinned allocation failed           */
+    VSFEEL_E_TIMEOUT = -5,  /* a bounded wait on the GPU expired            */
+    VSFEEL_E_FETCH = -6,    /* the frame callback returned no frame         */
+    VSFEEL_E_UNSUPPORTED = -7
+};
+
+/* Clip format, mirroring the VSVideoFormat fields the reference checks
+ * (src/bm3d.cpp:1085-1088, 1257-1275). */
+enum { VSFEEL_CF_GRAY = 1, VSFEEL_CF_YUV = 3 };
+enum { VSFEEL_ST_INTEGER = 0, VSFEEL_ST_FLOAT = 1 };
+
+typedef struct vsfeel_bm3d_video_info {
+    int width, height, num_frames;
+    int color_family;     /* VSFEEL_CF_GRAY or VSFEEL_CF_YUV             */
+    int sample_type;      /* VSFEEL_ST_FLOAT                              */
+    int bits_per_sample;  /* 32                                           */
+    int sub_sampling_w, sub_sampling_h;
+} vsfeel_bm3d_video_info;
+
+/* The BM3Dv2 argument map (registration string at src/bm3d.cpp:1562-1571).
+ * An array argument with count 0 is absent and takes the reference default;
+ * a missing element copies the previous one (src/bm3d.cpp:1090-1167).
+ * Only element [0] of each array is used, as in the reference. */
+typedef struct vsfeel_bm3d_args {
+    float sigma[3];      int sigma_count;       /* default 3.0  */
+    int block_step[3];   int block_step_count;  /* default 8    */
+    int bm_range[3];     int bm_range_count;    /* default 9    */
+    int radius;          int radius_set;        /* default 0    */
+    int ps_num[3];       int ps_num_count;      /* default 2    */
+    int ps_range[3];     int ps_range_count;    /* default 4    */
+    int num_streams;     int num_streams_set;   /* default 4    */
+    int extractor_exp;   int extractor_exp_set; /* default 0    */
+    int has_ref;         /* a "ref" clip was given (final Wiener pass)     */
+    const vsfeel_bm3d_video_info* ref_info;  /* its format, when has_ref */
+} vsfeel_bm3d_args;
+
+typedef struct vsfeel_bm3d vsfeel_bm3d;
+
+/* Fills args with "all arguments absent". */
+VSFEEL_API void vsfeel_bm3d_args_init(vsfeel_bm3d_args* args);
+
+/* BM3DCreate: validates the arguments exactly as the reference does and
+ * binds a CUDA device context (device ordinal `device`, normally 0). */
+VSFEEL_API int vsfeel_bm3d_create(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
+                       int device, vsfeel_bm3d** out);
+
+/* BM3DFree. Accepts NULL. */
+VSFEEL_API void vsfeel_bm3d_free(vsfeel_bm3d* ctx);
+
+/* arInitial: the source frames output n needs, [*first, *last]
+ * (n - 2r .. n + 2r clamped to the clip). */
+VSFEEL_API int vsfeel_bm3d_frame_range(const vsfeel_bm3d* ctx, int n, int* first, int* last);
+
+/* Frame source for vsfeel_bm3d_get_frame: returns the luma plane of frame
+ * n with its row stride in bytes, or NULL on failure; the pointer stays
+ * valid until release(user, n) is called. */
+typedef const float* (*vsfeel_fetch_fn)(void* user, int n, ptrdiff_t* stride_bytes);
+typedef void (*vsfeel_release_fn)(void* user, int n);
+
+/* arAllFramesReady: denoises output frame n into dst (luma plane). Frames
+ * are fetched through the callbacks only when not already resident. */
+VSFEEL_API int vsfeel_bm3d_get_frame(vsfeel_bm3d* ctx, int n, vsfeel_fetch_fn fetch,
+                          vsfeel_release_fn release, void* user, float* dst,
+                          ptrdiff_t dst_stride_bytes);
+
+/* Whole clip from host memory: src holds all num_frames luma planes
+ * (frame f at src + f*frame_stride_bytes, rows row_stride_bytes apart);
+ * writes output frames first .. first+count-1 to dst (same layout, frame 0
+ * of dst = output `first`). Pinned host buffers give the fastest copies. */
+VSFEEL_API int vsfeel_bm3d_process_host(vsfeel_bm3d* ctx, const float* src, ptrdiff_t src_frame_stride_bytes,
+                             ptrdiff_t src_row_stride_bytes, float* dst,
+                             ptrdiff_t dst_frame_stride_bytes, ptrdiff_t dst_row_stride_bytes,
+                             int first, int count);
+
+/* Whole clip already in device memory (strides in floats), enqueued on
+ * `stream` (a cudaStream_t; NULL = the context's own stream). Returns after
+ * the work is enqueued; synchronise the stream before reading dst. */
+VSFEEL_API int vsfeel_bm3d_process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
+                               int64_t src_row_stride, float* dst, int64_t dst_frame_stride,
+                               int64_t dst_row_stride, int first, int count, void* stream);
+
+/* Effective parameters after defaults and scaling (for callers and tests). */
+typedef struct vsfeel_bm3d_info {
+    int width, height, num_frames, radius, block_step, bm_range, ps_num, ps_range, num_streams;
+    float sigma;      /* user sigma[0]                                    */
+    float threshold;  /* sigma * 0x3f021bb6 (src/bm3d.cpp:1103-1113)      */
+    float extractor;  /* 2^extractor_exp, or 0 (src/bm3d.cpp:1188-1190)   */
+    int blocks_x, blocks_y;
+    int64_t device_bytes;  /* device memory held by the context           */
+} vsfeel_bm3d_info;
+
+VSFEEL_API int vsfeel_bm3d_get_info(const vsfeel_bm3d* ctx, vsfeel_bm3d_info* info);
+
+/* Match table of stack m (testing and the adjoint): table receives
+ * blocks_x*blocks_y*8 entries of (x, y, z) int32 triples, blocks in raster
+ * order, computed from the device frames given as in process_device. */
+VSFEEL_API int vsfeel_bm3d_match_table_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
+                                   int64_t src_row_stride, int m, int32_t* table_host);
+
+/* Kernel launches issued by this context since creation (all kernels). */
+VSFEEL_API int64_t vsfeel_bm3d_launch_count(const vsfeel_bm3d* ctx);
+
+/* The calling thread's last error message ("" when none). */
+VSFEEL_API const char* vsfeel_bm3d_last_error(void);
+
+/* ABI version of the loaded library (VSFEEL_BM3D_ABI_VERSION). */
+VSFEEL_API int vsfeel_bm3d_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VSFEEL_BM3D_H */

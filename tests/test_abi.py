@@ -1,0 +1,124 @@
+"""The C ABI library: loads, exports every declared symbol, and validates
+arguments like the reference's BM3DCreate (CPU only; no kernel runs)."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+import vsfeel
+from vsfeel import _lib
+
+
+def _declared_symbols() -> set[str]:
+    names = set()
+    for h in (ROOT / "include").glob("*.h"):
+        text = h.read_text()
+        names |= set(re.findall(r"VSFEEL_API\s+[\w\s\*]+?\b(vsfeel_\w+)\s*\(", text))
+    return names
+
+
+def test_header_declares_the_binding_exports():
+    assert _declared_symbols() == set(_lib.EXPORTS)
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    for name in _declared_symbols():
+        assert hasattr(lib, name), name
+    assert lib.vsfeel_bm3d_abi_version() == _lib.ABI_VERSION
+
+
+def test_library_exports_nothing_else():
+    import subprocess
+    out = subprocess.run(["nm", "-D", "--defined-only", str(_lib.LIB_PATH)], capture_output=True,
+                         text=True, check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.split()[-1].startswith("vsfeel")}
+    assert exported == _declared_symbols()
+
+
+def _create(clip_shape=(4, 32, 48), fmt=vsfeel.GRAYS, **kw):
+    clip = vsfeel.clip_from_array(np.zeros(clip_shape, np.float32), fmt=fmt)
+    return vsfeel.BM3Dv2(clip, **kw)
+
+
+@pytest.mark.parametrize("kwargs,message", [
+    (dict(sigma=-1.0), '"sigma" must be non-negative'),
+    (dict(sigma=[1.0, -0.5]), '"sigma" must be non-negative'),
+    (dict(block_step=0), '"block_step" must be in range [1, 8]'),
+    (dict(block_step=9), '"block_step" must be in range [1, 8]'),
+    (dict(bm_range=0), '"bm_range" must be positive'),
+    (dict(radius=5), '"radius" must be in range [0, 4]'),
+    (dict(radius=-1), '"radius" must be in range [0, 4]'),
+    (dict(ps_num=0), '"ps_num" must be in range [1, 8]'),
+    (dict(ps_num=9), '"ps_num" must be in range [1, 8]'),
+    (dict(ps_range=0), '"ps_range" must be positive'),
+    (dict(num_streams=0), '"num_streams" must be positive'),
+])
+def test_argument_validation_messages(kwargs, message):
+    # src/bm3d.cpp:1090-1190 (the reference's tests: test_bm3dv2_rejects_radius5)
+    with pytest.raises(vsfeel.Error, match=re.escape("BM3D: " + message)):
+        _create(**kwargs)
+
+
+def test_rejects_integer_formats():
+    # test_bm3dv2_rejects_gray8: only 32-bit float input
+    gray8 = vsfeel.VideoFormat(_lib.CF_GRAY, _lib.ST_INTEGER, 8, 0, 0)
+    with pytest.raises(vsfeel.Error, match="only constant format 32 bit float input supported"):
+        _create(fmt=gray8)
+
+
+def test_rejects_bad_ref_format():
+    # test_bm3dv2_rejects_bad_ref_format: a ref of other dimensions
+    clip = vsfeel.clip_from_array(np.zeros((4, 32, 48), np.float32))
+    bad = vsfeel.clip_from_array(np.zeros((4, 32, 49), np.float32))
+    with pytest.raises(vsfeel.Error, match='"ref" must be of the same dimensions as "clip"'):
+        vsfeel.BM3Dv2(clip, ref=bad)
+    shorter = vsfeel.clip_from_array(np.zeros((3, 32, 48), np.float32))
+    with pytest.raises(vsfeel.Error, match='"ref" must be of the same number of frames'):
+        vsfeel.BM3Dv2(clip, ref=shorter)
+    yuv = vsfeel.clip_from_array(np.zeros((4, 32, 48), np.float32), np.zeros((4, 16, 24), np.float32),
+                                 np.zeros((4, 16, 24), np.float32))
+    with pytest.raises(vsfeel.Error, match='"ref" must be of the same format as "clip"'):
+        vsfeel.BM3Dv2(clip, ref=yuv)
+
+
+def test_rejects_rgb():
+    rgb = vsfeel.VideoFormat(2, _lib.ST_FLOAT, 32, 0, 0)
+    with pytest.raises(vsfeel.Error, match="only Gray and YUV input"):
+        _create(fmt=rgb)
+
+
+def test_rejects_frames_below_block_size():
+    with pytest.raises(vsfeel.Error, match="at least 8x8"):
+        _create(clip_shape=(2, 7, 32))
+
+
+def test_valid_arguments_reach_the_device_check_without_a_gpu():
+    """On a machine without a GPU, valid arguments fail only at the device
+    probe: the whole validation passed."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(vsfeel.Error, match="no CUDA device"):
+        _create(sigma=[3.0], block_step=4, bm_range=16, radius=2, ps_num=2, ps_range=7,
+                num_streams=4, extractor_exp=2)
+
+
+def test_errors_are_per_thread_and_prefixed():
+    lib = _lib.load()
+    with pytest.raises(vsfeel.Error):
+        _create(radius=7)
+    assert _lib.last_error(lib).startswith("BM3D: ")
+
+
+def test_null_context_is_rejected():
+    lib = _lib.load()
+    lo, hi = ctypes.c_int(), ctypes.c_int()
+    assert lib.vsfeel_bm3d_frame_range(None, 0, ctypes.byref(lo), ctypes.byref(hi)) == _lib.E_ARG
+    lib.vsfeel_bm3d_free(None)
+    assert lib.vsfeel_bm3d_launch_count(None) == 0

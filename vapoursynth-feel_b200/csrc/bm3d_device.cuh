@@ -1,0 +1,154 @@
+// Device-side building blocks of the BM3Dv2 basic estimate for sm_100a.
+//
+// Every floating-point operation whose bits decide a block match or a
+// threshold is spelled with an explicit round-to-nearest intrinsic
+// (__fadd_rn, __fmul_rn, __fmaf_rn, ...), so the results do not depend on
+// nvcc's contraction flags and equal the reference's operation order:
+//   8-point DCT pair ............ src/bm3d.comp:91-181
+//   column SSD .................. src/bm3d.comp:266-275 (e += d*d fused)
+//   8-column reduction tree ..... src/bm3d.comp:280-282
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace vsfeel {
+
+constexpr int kMaxRadius = 4;
+constexpr int kMaxTW = 2 * kMaxRadius + 1;
+constexpr float kFltMax = 3.402823466e+38f;
+constexpr int kSeqSentinel = 0x7fffffff;
+
+// One stack: the reference blocks of frame m, searched in the slices
+// z = 0..2r (frame clamp(m - r + z)).
+struct StackJob {
+    const float* slice_frame[kMaxTW];  // frame of each slice (search and denoise clip)
+    float* slice_dst[kMaxTW];          // numerator plane of each slice's target; null = dropped
+    int64_t dst_plane;                 // floats from a numerator plane to its weight plane
+    int pitch;                         // floats per frame row (inputs)
+    int dst_pitch;                     // floats per accumulator row
+    int width, height;
+    int radius, step, bm_range, ps_num, ps_range;
+    int nbx, nby;                      // block grid
+    float thr;                         // hard threshold, sigma * 0x3f021bb6
+    float extractor;                   // 2^exp or 0
+    uint32_t* match_xy;                // [nblocks][8]: x | y << 16
+    uint32_t* match_z;                 // [nblocks]: 8 x 4-bit slice index
+};
+
+// Per-output normalisation: numerator plane read at aggregation step i.
+struct NormalizeJob {
+    const float* num[kMaxTW];
+    int64_t den_offset;  // floats from a numerator plane to its weight plane
+    int tw, width, height, src_pitch, out_pitch;
+    float* out;
+};
+
+// Host-side launchers (defined beside the kernels). Each returns the launch
+// status and enqueues on `stream`.
+cudaError_t launch_match(const StackJob& job, cudaStream_t stream);
+cudaError_t launch_filter(const StackJob& job, cudaStream_t stream);
+cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream);
+
+__host__ __device__ inline int block_count(int extent, int step) {
+    return (extent - 9 + 2 * step) / step;  // positions x0 = b*step < extent - 8 + step
+}
+
+// ---------------------------------------------------------------------------
+// 8-point DCT-II scaled x4 per axis, and its transpose. The statement order
+// and the fused operations are those of the reference codelet.
+__device__ __forceinline__ void dct8_fwd(float v[8]) {
+    const float c414 = 0.414213562373095048801688724209698078569671875;
+    const float c1847 = 1.847759065022573512256366378793576573644833252;
+    const float c198 = 0.198912367379658006911597622644676228597850501;
+    const float c1961 = 1.961570560806460898252364472268478073947867462;
+    const float c1414 = 1.414213562373095048801688724209698078569671875;
+    const float c668 = 0.668178637919298919997757686523080761552472251;
+    const float c1662 = 1.662939224605090474157576755235811513477121624;
+    const float c707 = 0.707106781186547524400844362104849039284835938;
+
+    const float d07 = __fsub_rn(v[0], v[7]), s07 = __fadd_rn(v[0], v[7]);
+    const float d43 = __fsub_rn(v[4], v[3]), s43 = __fadd_rn(v[4], v[3]);
+    const float d25 = __fsub_rn(v[2], v[5]);
+    const float d16 = __fsub_rn(v[1], v[6]);
+    const float a = __fadd_rn(d25, d16);
+    const float s16 = __fadd_rn(v[1], v[6]);
+    const float b = __fsub_rn(d25, d16);
+    const float s25 = __fadd_rn(v[2], v[5]);
+    const float p = __fmaf_rn(-c707, a, d07);
+    const float q = __fmaf_rn(-c707, b, d43);
+    v[3] = __fmul_rn(c1662, __fmaf_rn(c668, q, p));
+    v[5] = -__fmul_rn(c1662, __fmaf_rn(-c668, p, q));
+    const float e0 = __fadd_rn(s07, s43), e1 = __fadd_rn(s25, s16);
+    v[4] = __fmul_rn(c1414, __fsub_rn(e0, e1));
+    v[0] = __fmul_rn(c1414, __fadd_rn(e0, e1));
+    const float h = __fmaf_rn(c707, a, d07);
+    const float i = __fmaf_rn(c707, b, d43);
+    v[1] = __fmul_rn(c1961, __fmaf_rn(-c198, i, h));
+    v[7] = __fmul_rn(c1961, __fmaf_rn(c198, h, i));
+    const float l = __fsub_rn(s07, s43), o = __fsub_rn(s25, s16);
+    v[2] = __fmul_rn(c1847, __fmaf_rn(-c414, o, l));
+    v[6] = __fmul_rn(c1847, __fmaf_rn(c414, l, o));
+}
+
+__device__ __forceinline__ void dct8_inv(float v[8]) {
+    const float c1662 = 1.662939224605090474157576755235811513477121624;
+    const float c668 = 0.668178637919298919997757686523080761552472251;
+    const float c1961 = 1.961570560806460898252364472268478073947867462;
+    const float c198 = 0.198912367379658006911597622644676228597850501;
+    const float c1847 = 1.847759065022573512256366378793576573644833252;
+    const float c707 = 0.707106781186547524400844362104849039284835938;
+    const float c414 = 0.414213562373095048801688724209698078569671875;
+    const float c1414 = 1.414213562373095048801688724209698078569671875;
+
+    const float dc = __fmul_rn(v[0], c1414);
+    const float a = __fmaf_rn(c1414, v[4], dc);
+    const float b = __fmaf_rn(-c1414, v[4], dc);
+    const float c = __fmaf_rn(c414, v[6], v[2]);
+    const float d = __fmaf_rn(c414, v[2], -v[6]);
+    const float s53 = __fadd_rn(v[5], v[3]);
+    const float d35 = __fsub_rn(v[3], v[5]);
+    const float e = __fmaf_rn(c707, s53, v[1]);
+    const float f = __fmaf_rn(-c707, d35, v[7]);
+    const float g = __fmaf_rn(c707, d35, v[7]);
+    const float h = __fmaf_rn(-c707, s53, v[1]);
+    const float t0 = __fmaf_rn(c1847, c, a);
+    const float t1 = __fmaf_rn(c198, g, e);
+    const float t2 = __fmaf_rn(-c1847, d, b);
+    const float t3 = __fmaf_rn(c668, h, f);
+    const float t4 = __fmaf_rn(-c1847, c, a);
+    const float t5 = __fmaf_rn(-c198, e, g);
+    const float t6 = __fmaf_rn(c1847, d, b);
+    const float t7 = __fmaf_rn(-c668, f, h);
+    v[0] = __fmaf_rn(c1961, t1, t0);
+    v[7] = __fmaf_rn(-c1961, t1, t0);
+    v[2] = __fmaf_rn(c1662, t3, t2);
+    v[5] = __fmaf_rn(-c1662, t3, t2);
+    v[3] = __fmaf_rn(-c1961, t5, t4);
+    v[4] = __fmaf_rn(c1961, t5, t4);
+    v[6] = __fmaf_rn(-c1662, t7, t6);
+    v[1] = __fmaf_rn(c1662, t7, t6);
+}
+
+// ---------------------------------------------------------------------------
+// SSD of one 8-row column: block column `c` (8 values) against the source
+// column at (cy .. cy+7, X). Even and odd rows accumulate separately.
+__device__ __forceinline__ float column_ssd(const float cc[8], const float* __restrict__ col,
+                                            int pitch) {
+    float ev = 0.0f, od = 0.0f;
+#pragma unroll
+    for (int i = 0; i < 8; i += 2) {
+        const float d0 = __fsub_rn(cc[i], __ldg(col + (size_t)i * pitch));
+        ev = __fmaf_rn(d0, d0, ev);
+        const float d1 = __fsub_rn(cc[i + 1], __ldg(col + (size_t)(i + 1) * pitch));
+        od = __fmaf_rn(d1, d1, od);
+    }
+    return __fadd_rn(ev, od);
+}
+
+__device__ __forceinline__ float tree8(const float col[8]) {
+    return __fadd_rn(__fadd_rn(__fadd_rn(col[0], col[1]), __fadd_rn(col[2], col[3])),
+                     __fadd_rn(__fadd_rn(col[4], col[5]), __fadd_rn(col[6], col[7])));
+}
+
+}  // namespace vsfeel

@@ -1,0 +1,624 @@
+// Host side of the B200 BM3Dv2 basic estimate: the C ABI declared in
+// include/vsfeel_bm3d.h.
+//
+// Replaces the reference's Vulkan machinery (src/vsfeel.cpp, src/bm3d.cpp)
+// with one CUDA stream per context, device-resident frames and a ring of
+// per-output accumulator slots:
+//
+// * Stack m (the reference blocks of frame m) searches and filters in the
+//   slices z = 0..2r, slice z being frame clamp(m - r + z). Output frame n
+//   sums, in order i = 0..2r, slice agg_z(i, n) of stack clamp(n - r + i)
+//   (src/bm3d.cpp:369-371, 628-696). Each slice is therefore read by at most
+//   one output, n = clamp(m - r + z); slices no output reads are dropped.
+// * Output n owns a slot of TW (numerator, weight) plane pairs, one per
+//   contributing stack m = n - r + j. A stack scatters straight into its
+//   outputs' slots, so no per-stack result cache is needed; output n is
+//   normalised as soon as stack min(n + r, N - 1) is done, and its slot is
+//   reused by output n + 2r + 1.
+#include "bm3d_device.cuh"
+#include "../../include/vsfeel_bm3d.h"
+
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace {
+
+using namespace vsfeel;
+
+thread_local std::string g_error;
+
+int fail(int code, const std::string& msg) {
+    g_error = "BM3D: " + msg;
+    return code;
+}
+
+struct CudaError {
+    cudaError_t err;
+    const char* what;
+};
+
+#define VSF_CUDA(call)                                                       \
+    do {                                                                     \
+        cudaError_t e_ = (call);                                             \
+        if (e_ != cudaSuccess) throw CudaError{e_, #call};                   \
+    } while (0)
+
+inline int clampi(int v, int lo, int hi) { return std::min(std::max(v, lo), hi); }
+
+int agg_z(int i, int n, int nframes, int radius) {
+    return std::min(std::max(2 * radius - i, n - nframes + 1 + radius), n + radius);
+}
+
+float hard_factor() {
+    const uint32_t bits = 0x3f021bb6u;
+    float f;
+    std::memcpy(&f, &bits, 4);
+    return f;
+}
+
+int64_t timeout_ms() {
+    const char* s = std::getenv("VSFEEL_TIMEOUT_MS");
+    if (s && *s) {
+        const long long v = std::atoll(s);
+        if (v > 0) return v;
+    }
+    return 120000;
+}
+
+// Bounded wait on a stream: polls until idle or the deadline passes.
+int wait_stream(cudaStream_t s, int64_t limit_ms) {
+    const auto t0 = std::chrono::steady_clock::now();
+    int spins = 0;
+    for (;;) {
+        const cudaError_t e = cudaStreamQuery(s);
+        if (e == cudaSuccess) return VSFEEL_OK;
+        if (e != cudaErrorNotReady)
+            return fail(VSFEEL_E_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+        const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                            std::chrono::steady_clock::now() - t0)
+                            .count();
+        if (ms >= limit_ms)
+            return fail(VSFEEL_E_TIMEOUT, "timed out after " + std::to_string(ms) +
+                                              " ms waiting for the GPU");
+        if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+struct Settings {
+    int width = 0, height = 0, nframes = 0;
+    bool chroma = false;
+    float sigma = 3.0f, thr = 0.0f, extractor = 0.0f;
+    int step = 8, bm_range = 9, radius = 0, ps_num = 2, ps_range = 4, num_streams = 4;
+};
+
+// Argument parsing and validation in the order and with the messages of
+// BM3DCreate (src/bm3d.cpp:1062-1190, 1257-1275).
+int parse_args(const vsfeel_bm3d_args* a, const vsfeel_bm3d_video_info* vi, Settings& s) {
+    if (!a || !vi) return fail(VSFEEL_E_ARG, "null argument");
+    if (a->has_ref) {
+        const vsfeel_bm3d_video_info* r = a->ref_info;
+        if (!r) return fail(VSFEEL_E_ARG, "\"ref\" given without its format");
+        if (r->color_family != vi->color_family || r->sample_type != vi->sample_type ||
+            r->bits_per_sample != vi->bits_per_sample || r->sub_sampling_w != vi->sub_sampling_w ||
+            r->sub_sampling_h != vi->sub_sampling_h)
+            return fail(VSFEEL_E_ARG, "\"ref\" must be of the same format as \"clip\"");
+        if (r->width != vi->width || r->height != vi->height)
+            return fail(VSFEEL_E_ARG, "\"ref\" must be of the same dimensions as \"clip\"");
+        if (r->num_frames != vi->num_frames)
+            return fail(VSFEEL_E_ARG, "\"ref\" must be of the same number of frames as \"clip\"");
+    }
+    if (vi->width <= 0 || vi->height <= 0 || vi->sample_type != VSFEEL_ST_FLOAT ||
+        vi->bits_per_sample != 32)
+        return fail(VSFEEL_E_FORMAT, "only constant format 32 bit float input supported");
+
+    float sigma[3];
+    for (int i = 0; i < 3; ++i) {
+        if (i < a->sigma_count) {
+            sigma[i] = a->sigma[i];
+            if (sigma[i] < 0.0f) return fail(VSFEEL_E_ARG, "\"sigma\" must be non-negative");
+        } else {
+            sigma[i] = i == 0 ? 3.0f : sigma[i - 1];
+        }
+    }
+    int step[3], bmr[3], psn[3], psr[3];
+    for (int i = 0; i < 3; ++i) {
+        if (i < a->block_step_count) {
+            step[i] = a->block_step[i];
+            if (step[i] <= 0 || step[i] > 8)
+                return fail(VSFEEL_E_ARG, "\"block_step\" must be in range [1, 8]");
+        } else {
+            step[i] = i == 0 ? 8 : step[i - 1];
+        }
+    }
+    for (int i = 0; i < 3; ++i) {
+        if (i < a->bm_range_count) {
+            bmr[i] = a->bm_range[i];
+            if (bmr[i] <= 0) return fail(VSFEEL_E_ARG, "\"bm_range\" must be positive");
+        } else {
+            bmr[i] = i == 0 ? 9 : bmr[i - 1];
+        }
+    }
+    s.radius = a->radius_set ? a->radius : 0;
+    if (s.radius < 0 || s.radius > kMaxRadius)
+        return fail(VSFEEL_E_ARG, "\"radius\" must be in range [0, 4]");
+    for (int i = 0; i < 3; ++i) {
+        if (i < a->ps_num_count) {
+            psn[i] = a->ps_num[i];
+            if (psn[i] <= 0 || psn[i] > 8)
+                return fail(VSFEEL_E_ARG, "\"ps_num\" must be in range [1, 8]");
+        } else {
+            psn[i] = i == 0 ? 2 : psn[i - 1];
+        }
+    }
+    for (int i = 0; i < 3; ++i) {
+        if (i < a->ps_range_count) {
+            psr[i] = a->ps_range[i];
+            if (psr[i] <= 0) return fail(VSFEEL_E_ARG, "\"ps_range\" must be positive");
+        } else {
+            psr[i] = i == 0 ? 4 : psr[i - 1];
+        }
+    }
+    s.num_streams = a->num_streams_set ? a->num_streams : 4;
+    if (s.num_streams <= 0) return fail(VSFEEL_E_ARG, "\"num_streams\" must be positive");
+    const int ext = a->extractor_exp_set ? a->extractor_exp : 0;
+
+    s.sigma = sigma[0];
+    s.thr = sigma[0] * hard_factor();
+    s.extractor = ext != 0 ? std::ldexp(1.0f, ext) : 0.0f;
+    s.step = step[0];
+    s.bm_range = bmr[0];
+    s.ps_num = psn[0];
+    s.ps_range = psr[0];
+    s.width = vi->width;
+    s.height = vi->height;
+    s.nframes = vi->num_frames;
+
+    if (vi->color_family == VSFEEL_CF_GRAY) {
+        s.chroma = false;
+    } else if (vi->color_family == VSFEEL_CF_YUV) {
+        s.chroma = true;
+    } else {
+        return fail(VSFEEL_E_FORMAT, "only Gray and YUV input are currently supported");
+    }
+    if (a->has_ref)
+        return fail(VSFEEL_E_UNSUPPORTED,
+                    "the final (Wiener) pass with \"ref\" is not supported by this build");
+    // The reference reads outside the plane below 8x8; the match table packs
+    // coordinates in 16 bits.
+    if (s.width < 8 || s.height < 8)
+        return fail(VSFEEL_E_FORMAT, "clip dimensions must be at least 8x8");
+    if (s.width > 65535 || s.height > 65535)
+        return fail(VSFEEL_E_FORMAT, "clip dimensions must be at most 65535");
+    if (s.nframes <= 0) return fail(VSFEEL_E_FORMAT, "clip must have at least one frame");
+    return VSFEEL_OK;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    void ensure(size_t count) {
+        if (count <= n) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+        VSF_CUDA(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+}  // namespace
+
+struct vsfeel_bm3d {
+    Settings s;
+    int device = 0;
+    int nbx = 0, nby = 0, nblocks = 0;
+    int acc_pitch = 0;       // floats per accumulator / staged frame row
+    size_t acc_plane = 0;    // floats per accumulator plane
+    cudaStream_t stream = nullptr;
+    std::mutex lock;
+    std::atomic<int64_t> launches{0};
+
+    DevBuf<float> ring;       // (2r+1) slots x TW x {num, den} planes
+    DevBuf<uint32_t> match_xy;
+    DevBuf<uint32_t> match_z;
+    DevBuf<float> frames;     // staged input frames (host and frame paths)
+    DevBuf<float> outbuf;     // staged output frames (host and frame paths)
+    std::map<int, int> frame_slot;  // frame cache of the per-frame path
+    std::vector<int> slot_frame;
+
+    int tw() const { return 2 * s.radius + 1; }
+    int clampf(int f) const { return clampi(f, 0, s.nframes - 1); }
+
+    size_t ring_floats() const { return (size_t)tw() * tw() * 2 * acc_plane; }
+    float* slot_pair(int n, int j) {
+        const int slot = n % tw();
+        return ring.p + ((size_t)slot * tw() + j) * 2 * acc_plane;
+    }
+
+    // The slice of stack m that output n reads (n = clamp(m - r + z)).
+    int read_slice(int n, int m) const {
+        const int r = s.radius;
+        for (int i = 0; i < tw(); ++i)
+            if (clampf(n - r + i) == m) return (r == 0) ? 0 : agg_z(i, n, s.nframes, r);
+        return -1;
+    }
+
+    void launch_stack(int m, const std::function<const float*(int)>& frame_ptr, int in_pitch,
+                      int out_lo, int out_hi, cudaStream_t st) {
+        const int r = s.radius;
+        StackJob job{};
+        for (int z = 0; z < tw(); ++z) {
+            job.slice_frame[z] = frame_ptr(clampf(m - r + z));
+            const int n = clampf(m - r + z);
+            job.slice_dst[z] = nullptr;
+            if (n >= out_lo && n <= out_hi && read_slice(n, m) == z)
+                job.slice_dst[z] = slot_pair(n, m - (n - r));
+        }
+        job.dst_plane = (int64_t)acc_plane;
+        job.pitch = in_pitch;
+        job.dst_pitch = acc_pitch;
+        job.width = s.width;
+        job.height = s.height;
+        job.radius = r;
+        job.step = s.step;
+        job.bm_range = s.bm_range;
+        job.ps_num = s.ps_num;
+        job.ps_range = s.ps_range;
+        job.nbx = nbx;
+        job.nby = nby;
+        job.thr = s.thr;
+        job.extractor = s.extractor;
+        job.match_xy = match_xy.p;
+        job.match_z = match_z.p;
+        VSF_CUDA(launch_match(job, st));
+        VSF_CUDA(launch_filter(job, st));
+        launches += 2;
+    }
+
+    void launch_normalize(int n, float* out, int out_pitch, cudaStream_t st) {
+        const int r = s.radius;
+        NormalizeJob job{};
+        for (int i = 0; i < tw(); ++i) {
+            const int m = clampf(n - r + i);
+            job.num[i] = slot_pair(n, m - (n - r));
+        }
+        job.den_offset = (int64_t)acc_plane;
+        job.tw = tw();
+        job.width = s.width;
+        job.height = s.height;
+        job.src_pitch = acc_pitch;
+        job.out_pitch = out_pitch;
+        job.out = out;
+        VSF_CUDA(vsfeel::launch_normalize(job, st));
+        launches += 1;
+    }
+
+    // Denoises outputs [first, first+count) from device frames.
+    void run(const std::function<const float*(int)>& frame_ptr, int in_pitch,
+             const std::function<float*(int)>& out_ptr, int out_pitch, int first, int count,
+             cudaStream_t st) {
+        if (count <= 0) return;
+        const int r = s.radius;
+        const int last = first + count - 1;
+        ring.ensure(ring_floats());
+        match_xy.ensure((size_t)nblocks * 8);
+        match_z.ensure((size_t)nblocks);
+        const int m_lo = clampf(first - r), m_hi = clampf(last + r);
+        int zeroed = first - 1;     // highest output whose slot is zeroed
+        int finished = first - 1;   // highest output normalised
+        for (int m = m_lo; m <= m_hi; ++m) {
+            const int want = std::min(last, m + r);
+            for (int n = zeroed + 1; n <= want; ++n)
+                VSF_CUDA(cudaMemsetAsync(slot_pair(n, 0), 0,
+                                         sizeof(float) * (size_t)tw() * 2 * acc_plane, st));
+            zeroed = std::max(zeroed, want);
+            launch_stack(m, frame_ptr, in_pitch, first, last, st);
+            const int done = (m == m_hi) ? last : std::min(last, m - r);
+            for (int n = finished + 1; n <= done; ++n) launch_normalize(n, out_ptr(n), out_pitch, st);
+            finished = std::max(finished, done);
+        }
+    }
+
+    size_t frame_floats() const { return (size_t)s.height * acc_pitch; }
+};
+
+namespace {
+
+template <class F>
+int guarded(vsfeel_bm3d* ctx, F&& fn) {
+    if (!ctx) return fail(VSFEEL_E_ARG, "null context");
+    std::lock_guard<std::mutex> lk(ctx->lock);
+    DeviceGuard dg(ctx->device);
+    try {
+        return fn();
+    } catch (const CudaError& e) {
+        if (e.err == cudaErrorMemoryAllocation) {
+            cudaGetLastError();
+            return fail(VSFEEL_E_MEMORY, std::string("out of device memory (") + e.what + ")");
+        }
+        return fail(VSFEEL_E_CUDA,
+                    std::string("CUDA error: ") + cudaGetErrorString(e.err) + " (" + e.what + ")");
+    } catch (const std::bad_alloc&) {
+        return fail(VSFEEL_E_MEMORY, "out of host memory");
+    } catch (const std::exception& e) {
+        return fail(VSFEEL_E_ARG, std::string("internal error: ") + e.what());
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int vsfeel_bm3d_abi_version(void) { return VSFEEL_BM3D_ABI_VERSION; }
+
+const char* vsfeel_bm3d_last_error(void) { return g_error.c_str(); }
+
+void vsfeel_bm3d_args_init(vsfeel_bm3d_args* a) {
+    if (a) std::memset(a, 0, sizeof(*a));
+}
+
+int vsfeel_bm3d_create(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi, int device,
+                       vsfeel_bm3d** out) {
+    g_error.clear();
+    if (!out) return fail(VSFEEL_E_ARG, "null output pointer");
+    *out = nullptr;
+    Settings s;
+    const int rc = parse_args(args, vi, s);
+    if (rc != VSFEEL_OK) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return fail(VSFEEL_E_CUDA, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(VSFEEL_E_ARG, "invalid device ordinal");
+    auto* ctx = new (std::nothrow) vsfeel_bm3d();
+    if (!ctx) return fail(VSFEEL_E_MEMORY, "out of host memory");
+    ctx->s = s;
+    ctx->device = device;
+    ctx->nbx = block_count(s.width, s.step);
+    ctx->nby = block_count(s.height, s.step);
+    ctx->nblocks = ctx->nbx * ctx->nby;
+    ctx->acc_pitch = (s.width + 31) & ~31;
+    ctx->acc_plane = (size_t)s.height * ctx->acc_pitch;
+    DeviceGuard dg(device);
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete ctx;
+        return fail(VSFEEL_E_CUDA, "could not create a CUDA stream");
+    }
+    *out = ctx;
+    return VSFEEL_OK;
+}
+
+void vsfeel_bm3d_free(vsfeel_bm3d* ctx) {
+    if (!ctx) return;
+    {
+        DeviceGuard dg(ctx->device);
+        if (ctx->stream) {
+            wait_stream(ctx->stream, timeout_ms());
+            cudaStreamDestroy(ctx->stream);
+        }
+        ctx->ring.release();
+        ctx->match_xy.release();
+        ctx->match_z.release();
+        ctx->frames.release();
+        ctx->outbuf.release();
+    }
+    delete ctx;
+}
+
+int vsfeel_bm3d_frame_range(const vsfeel_bm3d* ctx, int n, int* first, int* last) {
+    if (!ctx || !first || !last) return fail(VSFEEL_E_ARG, "null argument");
+    if (n < 0 || n >= ctx->s.nframes) return fail(VSFEEL_E_ARG, "frame index out of range");
+    const int r = ctx->s.radius;
+    *first = clampi(n - 2 * r, 0, ctx->s.nframes - 1);
+    *last = clampi(n + 2 * r, 0, ctx->s.nframes - 1);
+    return VSFEEL_OK;
+}
+
+int vsfeel_bm3d_get_info(const vsfeel_bm3d* ctx, vsfeel_bm3d_info* info) {
+    if (!ctx || !info) return fail(VSFEEL_E_ARG, "null argument");
+    const Settings& s = ctx->s;
+    info->width = s.width;
+    info->height = s.height;
+    info->num_frames = s.nframes;
+    info->radius = s.radius;
+    info->block_step = s.step;
+    info->bm_range = s.bm_range;
+    info->ps_num = s.ps_num;
+    info->ps_range = s.ps_range;
+    info->num_streams = s.num_streams;
+    info->sigma = s.sigma;
+    info->threshold = s.thr;
+    info->extractor = s.extractor;
+    info->blocks_x = ctx->nbx;
+    info->blocks_y = ctx->nby;
+    info->device_bytes = (int64_t)(ctx->ring.n + ctx->frames.n + ctx->outbuf.n) * 4 +
+                         (int64_t)(ctx->match_xy.n + ctx->match_z.n) * 4;
+    return VSFEEL_OK;
+}
+
+int64_t vsfeel_bm3d_launch_count(const vsfeel_bm3d* ctx) { return ctx ? ctx->launches.load() : 0; }
+
+int vsfeel_bm3d_process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
+                               int64_t src_row_stride, float* dst, int64_t dst_frame_stride,
+                               int64_t dst_row_stride, int first, int count, void* stream) {
+    return guarded(ctx, [&]() -> int {
+        const Settings& s = ctx->s;
+        if (!src || !dst) return fail(VSFEEL_E_ARG, "null frame buffer");
+        if (first < 0 || count < 0 || first + count > s.nframes)
+            return fail(VSFEEL_E_ARG, "output range outside the clip");
+        if (src_row_stride < s.width || dst_row_stride < s.width || src_row_stride > INT32_MAX ||
+            dst_row_stride > INT32_MAX)
+            return fail(VSFEEL_E_ARG, "row stride smaller than the width");
+        if (src_frame_stride < src_row_stride * s.height || dst_frame_stride < dst_row_stride * s.height)
+            return fail(VSFEEL_E_ARG, "frame stride smaller than a plane");
+        cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+        ctx->run([&](int f) { return src + (size_t)f * src_frame_stride; }, (int)src_row_stride,
+                 [&](int n) { return dst + (size_t)(n - first) * dst_frame_stride; },
+                 (int)dst_row_stride, first, count, st);
+        return VSFEEL_OK;
+    });
+}
+
+int vsfeel_bm3d_process_host(vsfeel_bm3d* ctx, const float* src, ptrdiff_t src_frame_stride_bytes,
+                             ptrdiff_t src_row_stride_bytes, float* dst,
+                             ptrdiff_t dst_frame_stride_bytes, ptrdiff_t dst_row_stride_bytes,
+                             int first, int count) {
+    return guarded(ctx, [&]() -> int {
+        const Settings& s = ctx->s;
+        if (!src || !dst) return fail(VSFEEL_E_ARG, "null frame buffer");
+        if (first < 0 || count < 0 || first + count > s.nframes)
+            return fail(VSFEEL_E_ARG, "output range outside the clip");
+        const size_t row_bytes = sizeof(float) * (size_t)s.width;
+        if (src_row_stride_bytes < (ptrdiff_t)row_bytes || dst_row_stride_bytes < (ptrdiff_t)row_bytes)
+            return fail(VSFEEL_E_ARG, "row stride smaller than the width");
+        if (count == 0) return VSFEEL_OK;
+        const int r = s.radius;
+        const int f_lo = ctx->clampf(first - 2 * r), f_hi = ctx->clampf(first + count - 1 + 2 * r);
+        const int nin = f_hi - f_lo + 1;
+        const size_t ff = ctx->frame_floats();
+        ctx->frame_slot.clear();
+        ctx->slot_frame.clear();
+        ctx->frames.ensure(ff * nin);
+        ctx->outbuf.ensure(ff * count);
+        cudaStream_t st = ctx->stream;
+        for (int f = f_lo; f <= f_hi; ++f)
+            VSF_CUDA(cudaMemcpy2DAsync(ctx->frames.p + (size_t)(f - f_lo) * ff,
+                                       sizeof(float) * ctx->acc_pitch,
+                                       (const char*)src + (ptrdiff_t)f * src_frame_stride_bytes,
+                                       src_row_stride_bytes, row_bytes, s.height,
+                                       cudaMemcpyHostToDevice, st));
+        ctx->run([&](int f) { return ctx->frames.p + (size_t)(f - f_lo) * ff; }, ctx->acc_pitch,
+                 [&](int n) { return ctx->outbuf.p + (size_t)(n - first) * ff; }, ctx->acc_pitch,
+                 first, count, st);
+        for (int q = 0; q < count; ++q)
+            VSF_CUDA(cudaMemcpy2DAsync((char*)dst + (ptrdiff_t)q * dst_frame_stride_bytes,
+                                       dst_row_stride_bytes, ctx->outbuf.p + (size_t)q * ff,
+                                       sizeof(float) * ctx->acc_pitch, row_bytes, s.height,
+                                       cudaMemcpyDeviceToHost, st));
+        return wait_stream(st, timeout_ms());
+    });
+}
+
+int vsfeel_bm3d_get_frame(vsfeel_bm3d* ctx, int n, vsfeel_fetch_fn fetch, vsfeel_release_fn release,
+                          void* user, float* dst, ptrdiff_t dst_stride_bytes) {
+    return guarded(ctx, [&]() -> int {
+        const Settings& s = ctx->s;
+        if (!fetch || !dst) return fail(VSFEEL_E_ARG, "null callback or destination");
+        if (n < 0 || n >= s.nframes) return fail(VSFEEL_E_ARG, "frame index out of range");
+        const size_t row_bytes = sizeof(float) * (size_t)s.width;
+        if (dst_stride_bytes < (ptrdiff_t)row_bytes)
+            return fail(VSFEEL_E_ARG, "row stride smaller than the width");
+        const int r = s.radius;
+        const int f_lo = ctx->clampf(n - 2 * r), f_hi = ctx->clampf(n + 2 * r);
+        const int cap = 4 * r + 2;  // window plus one frame of slack
+        const size_t ff = ctx->frame_floats();
+        if ((int)ctx->slot_frame.size() != cap) {
+            ctx->frame_slot.clear();
+            ctx->slot_frame.assign(cap, -1);
+        }
+        ctx->frames.ensure(ff * cap);
+        ctx->outbuf.ensure(ff);
+        cudaStream_t st = ctx->stream;
+        // evict cached frames outside the window, then upload the missing ones
+        for (auto it = ctx->frame_slot.begin(); it != ctx->frame_slot.end();) {
+            if (it->first < f_lo || it->first > f_hi) {
+                ctx->slot_frame[it->second] = -1;
+                it = ctx->frame_slot.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        for (int f = f_lo; f <= f_hi; ++f) {
+            if (ctx->frame_slot.count(f)) continue;
+            int slot = 0;
+            while (ctx->slot_frame[slot] != -1) ++slot;
+            ptrdiff_t stride = 0;
+            const float* p = fetch(user, f, &stride);
+            if (!p) return fail(VSFEEL_E_FETCH, "could not fetch source frame " + std::to_string(f));
+            if (stride < (ptrdiff_t)row_bytes) {
+                if (release) release(user, f);
+                return fail(VSFEEL_E_ARG, "source row stride smaller than the width");
+            }
+            VSF_CUDA(cudaMemcpy2DAsync(ctx->frames.p + (size_t)slot * ff,
+                                       sizeof(float) * ctx->acc_pitch, p, stride, row_bytes,
+                                       s.height, cudaMemcpyHostToDevice, st));
+            // the source frame must stay valid until the copy has run
+            const int wrc = wait_stream(st, timeout_ms());
+            if (release) release(user, f);
+            if (wrc != VSFEEL_OK) return wrc;
+            ctx->slot_frame[slot] = f;
+            ctx->frame_slot[f] = slot;
+        }
+        ctx->run([&](int f) { return ctx->frames.p + (size_t)ctx->frame_slot.at(f) * ff; },
+                 ctx->acc_pitch, [&](int) { return ctx->outbuf.p; }, ctx->acc_pitch, n, 1, st);
+        VSF_CUDA(cudaMemcpy2DAsync(dst, dst_stride_bytes, ctx->outbuf.p, sizeof(float) * ctx->acc_pitch,
+                                   row_bytes, s.height, cudaMemcpyDeviceToHost, st));
+        return wait_stream(st, timeout_ms());
+    });
+}
+
+int vsfeel_bm3d_match_table_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
+                                   int64_t src_row_stride, int m, int32_t* table_host) {
+    return guarded(ctx, [&]() -> int {
+        const Settings& s = ctx->s;
+        if (!src || !table_host) return fail(VSFEEL_E_ARG, "null argument");
+        if (m < 0 || m >= s.nframes) return fail(VSFEEL_E_ARG, "stack index out of range");
+        if (src_row_stride < s.width || src_row_stride > INT32_MAX)
+            return fail(VSFEEL_E_ARG, "row stride smaller than the width");
+        ctx->ring.ensure(ctx->ring_floats());
+        ctx->match_xy.ensure((size_t)ctx->nblocks * 8);
+        ctx->match_z.ensure((size_t)ctx->nblocks);
+        cudaStream_t st = ctx->stream;
+        // outputs range empty: the filter runs but every slice is dropped
+        ctx->launch_stack(m, [&](int f) { return src + (size_t)f * src_frame_stride; },
+                          (int)src_row_stride, 1, 0, st);
+        std::vector<uint32_t> xy((size_t)ctx->nblocks * 8), zz((size_t)ctx->nblocks);
+        VSF_CUDA(cudaMemcpyAsync(xy.data(), ctx->match_xy.p, xy.size() * 4, cudaMemcpyDeviceToHost, st));
+        VSF_CUDA(cudaMemcpyAsync(zz.data(), ctx->match_z.p, zz.size() * 4, cudaMemcpyDeviceToHost, st));
+        const int rc = wait_stream(st, timeout_ms());
+        if (rc != VSFEEL_OK) return rc;
+        for (int b = 0; b < ctx->nblocks; ++b)
+            for (int k = 0; k < 8; ++k) {
+                const uint32_t v = xy[(size_t)b * 8 + k];
+                table_host[((size_t)b * 8 + k) * 3 + 0] = (int32_t)(v & 0xffffu);
+                table_host[((size_t)b * 8 + k) * 3 + 1] = (int32_t)(v >> 16);
+                table_host[((size_t)b * 8 + k) * 3 + 2] = (int32_t)((zz[b] >> (4 * k)) & 15u);
+            }
+        return VSFEEL_OK;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,430 @@
+// sm_100a kernels of the BM3Dv2 basic estimate (hard-thresholding pass).
+//
+//   bm3d_match_kernel ..... block matching: spatial window, temporal
+//                           predictive search, forced self-match
+//                           (src/bm3d.comp:460-663); writes the match table
+//   bm3d_filter_kernel .... gather, 3D DCT, hard threshold, inverse and the
+//                           extractor-biased scatter into the output slices
+//                           (src/bm3d.comp:358-399, 666-716)
+//   bm3d_normalize_kernel . per-pixel FP64 sum over the TW slices and the
+//                           division (src/bm3d_agg.comp:36-52)
+//
+// Lane layout of the matching and filtering kernels: 8 lanes per reference
+// block, 4 blocks per warp. In matching, lane s scans the candidate rows
+// top+s, top+s+8, ... (stride-8 linear order at radius >= 3) into its own
+// sorted top-8; the 8 lists are merged with warp shuffles. Candidates are
+// ordered by (SSD, scan index), so the merged list is the 8 smallest keys,
+// exactly as in the reference.
+#include "bm3d_device.cuh"
+
+namespace vsfeel {
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint32_t pack_xy(int x, int y) {
+    return (uint32_t)x | ((uint32_t)y << 16);
+}
+
+struct LaneTop8 {
+    float e[8];
+    uint32_t xy[8];
+    int s[8];
+
+    __device__ __forceinline__ void reset() {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            e[k] = kFltMax;
+            xy[k] = 0;
+            s[k] = kSeqSentinel;
+        }
+    }
+
+    // strict `<`: an equal later candidate stays behind (src/bm3d.comp:284-302)
+    __device__ __forceinline__ void insert(float err, uint32_t cxy, int seq) {
+        if (err < e[7]) {
+#pragma unroll
+            for (int k = 7; k > 0; --k) {
+                const bool sh = err < e[k - 1];
+                const bool pl = err < e[k];
+                e[k] = sh ? e[k - 1] : (pl ? err : e[k]);
+                xy[k] = sh ? xy[k - 1] : (pl ? cxy : xy[k]);
+                s[k] = sh ? s[k - 1] : (pl ? seq : s[k]);
+            }
+            const bool p0 = err < e[0];
+            e[0] = p0 ? err : e[0];
+            xy[0] = p0 ? cxy : xy[0];
+            s[0] = p0 ? seq : s[0];
+        }
+    }
+};
+
+// Merge the 8 lane lists of this lane's group (lanes 8g..8g+7) into the 8
+// smallest (error, seq) keys; every lane of the group receives the result.
+// Ties between sentinels resolve to the lower lane, as in
+// src/bm3d.comp:324-356.
+__device__ __forceinline__ void merge_group(LaneTop8 L, float me[8], uint32_t mxy[8]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        float e = L.e[0];
+        int s = L.s[0];
+        int src = lane;
+#pragma unroll
+        for (int off = 1; off < 8; off <<= 1) {
+            const float oe = __shfl_xor_sync(kFull, e, off);
+            const int os = __shfl_xor_sync(kFull, s, off);
+            const int osrc = __shfl_xor_sync(kFull, src, off);
+            const bool take = oe < e || (oe == e && (os < s || (os == s && osrc < src)));
+            e = take ? oe : e;
+            s = take ? os : s;
+            src = take ? osrc : src;
+        }
+        me[k] = e;
+        mxy[k] = __shfl_sync(kFull, L.xy[0], src);
+        if (lane == src) {
+#pragma unroll
+            for (int q = 0; q < 7; ++q) {
+                L.e[q] = L.e[q + 1];
+                L.xy[q] = L.xy[q + 1];
+                L.s[q] = L.s[q + 1];
+            }
+            L.e[7] = kFltMax;
+            L.xy[7] = 0;
+            L.s[7] = kSeqSentinel;
+        }
+    }
+}
+
+// Scan one search window into this lane's list (src/bm3d.comp:493-526).
+// kSliding (radius < 3): the reference's sliding column scan, whose slot c
+// holds source column cx+c against block column min(c + cx-left, 7).
+template <bool kSliding>
+__device__ __forceinline__ void scan_window(const float cur[64], const float* __restrict__ f,
+                                            int pitch, int left, int right, int top, int bottom,
+                                            int seq_base, int sub, LaneTop8& L) {
+    const int rw = right - left + 1;
+    if (kSliding) {
+        for (int cy = top + sub; cy <= bottom; cy += 8) {
+            const float* row = f + (size_t)cy * pitch;
+            float col[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) col[c] = column_ssd(&cur[c * 8], row + left + c, pitch);
+            int seq = seq_base + (cy - top) * rw;
+            L.insert(tree8(col), pack_xy(left, cy), seq);
+            for (int cx = left + 1; cx <= right; ++cx) {
+#pragma unroll
+                for (int c = 0; c < 7; ++c) col[c] = col[c + 1];
+                col[7] = column_ssd(&cur[56], row + cx + 7, pitch);
+                ++seq;
+                L.insert(tree8(col), pack_xy(cx, cy), seq);
+            }
+        }
+    } else {
+        const int total = (bottom - top + 1) * rw;
+        int cy = top + sub / rw;
+        int cx = left + sub % rw;
+        for (int idx = sub; idx < total; idx += 8) {
+            const float* p = f + (size_t)cy * pitch + cx;
+            float col[8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) col[c] = column_ssd(&cur[c * 8], p + c, pitch);
+            L.insert(tree8(col), pack_xy(cx, cy), seq_base + idx);
+            cx += 8;
+            while (cx > right) {
+                cx -= rw;
+                cy += 1;
+            }
+        }
+    }
+}
+
+// global list insertion of a temporal match (src/bm3d.comp:304-322)
+__device__ __forceinline__ void ginsert(float ge[8], uint32_t gxy[8], int gz[8], float err,
+                                        uint32_t cxy, int cz) {
+    if (err < ge[7]) {
+#pragma unroll
+        for (int k = 7; k > 0; --k) {
+            const bool sh = err < ge[k - 1];
+            const bool pl = err < ge[k];
+            ge[k] = sh ? ge[k - 1] : (pl ? err : ge[k]);
+            gxy[k] = sh ? gxy[k - 1] : (pl ? cxy : gxy[k]);
+            gz[k] = sh ? gz[k - 1] : (pl ? cz : gz[k]);
+        }
+        const bool p0 = err < ge[0];
+        ge[0] = p0 ? err : ge[0];
+        gxy[0] = p0 ? cxy : gxy[0];
+        gz[0] = p0 ? cz : gz[0];
+    }
+}
+
+}  // namespace
+
+template <bool kSliding>
+__global__ void __launch_bounds__(128) bm3d_match_kernel(const StackJob job) {
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & 7;
+    const int nblocks = job.nbx * job.nby;
+    const int gblock = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
+    const bool valid = gblock < nblocks;
+    const int b = valid ? gblock : nblocks - 1;
+    const int by = b / job.nbx;
+    const int bx = b - by * job.nbx;
+    const int x = min(bx * job.step, job.width - 8);
+    const int y = min(by * job.step, job.height - 8);
+    const int r = job.radius;
+    const int pitch = job.pitch;
+    const float* __restrict__ fc = job.slice_frame[r];
+
+    float cur[64];
+#pragma unroll
+    for (int c = 0; c < 8; ++c)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) cur[c * 8 + i] = __ldg(fc + (size_t)(y + i) * pitch + x + c);
+
+    float ge[8];
+    uint32_t gxy[8];
+    int gz[8];
+    {
+        LaneTop8 L;
+        L.reset();
+        const int R = job.bm_range;
+        const int left = max(x - R, 0), right = min(x + R, job.width - 8);
+        const int top = max(y - R, 0), bottom = min(y + R, job.height - 8);
+        scan_window<kSliding>(cur, fc, pitch, left, right, top, bottom, 0, sub, L);
+        merge_group(L, ge, gxy);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) gz[k] = r;
+    }
+
+    // temporal predictive search (src/bm3d.comp:540-637): the spatial top-8
+    // seeds both directions; each frame's merged top-8 seeds the next frame
+    const int Q = job.ps_range;
+    const int area = (2 * Q + 1) * (2 * Q + 1);
+    uint32_t sxy[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) sxy[k] = gxy[k];
+    for (int dir = -1; dir <= 1; dir += 2) {
+        uint32_t pxy[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) pxy[k] = sxy[k];
+        for (int t = 1; t <= r; ++t) {
+            const int z = r + dir * t;
+            const float* __restrict__ ft = job.slice_frame[z];
+            LaneTop8 L;
+            L.reset();
+            for (int i = 0; i < job.ps_num; ++i) {
+                uint32_t p = pxy[0];
+#pragma unroll
+                for (int k = 1; k < 8; ++k) p = (i == k) ? pxy[k] : p;
+                const int pxi = (int)(p & 0xffffu), pyi = (int)(p >> 16);
+                const int left = max(pxi - Q, 0), right = min(pxi + Q, job.width - 8);
+                const int top = max(pyi - Q, 0), bottom = min(pyi + Q, job.height - 8);
+                scan_window<kSliding>(cur, ft, pitch, left, right, top, bottom, i * area, sub, L);
+            }
+            float fe[8];
+            uint32_t fxy[8];
+            merge_group(L, fe, fxy);
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if (i < job.ps_num) ginsert(ge, gxy, gz, fe[i], fxy[i], z);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) pxy[k] = fxy[k];
+        }
+    }
+
+    // forced self-match (src/bm3d.comp:639-663)
+    const uint32_t self_xy = pack_xy(x, y);
+    bool has_self = false;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) has_self = has_self || (gxy[k] == self_xy && gz[k] == r);
+    if (!has_self) {
+#pragma unroll
+        for (int k = 7; k > 0; --k) {
+            gxy[k] = gxy[k - 1];
+            gz[k] = gz[k - 1];
+        }
+        gxy[0] = self_xy;
+        gz[0] = r;
+    }
+
+    if (valid && sub == 0) {
+        uint4* dst = reinterpret_cast<uint4*>(job.match_xy + (size_t)b * 8);
+        dst[0] = make_uint4(gxy[0], gxy[1], gxy[2], gxy[3]);
+        dst[1] = make_uint4(gxy[4], gxy[5], gxy[6], gxy[7]);
+        uint32_t zp = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) zp |= (uint32_t)gz[k] << (4 * k);
+        job.match_z[b] = zp;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Filtering. Lane sub of a group holds column sub of the 8 matched patches:
+// d[k*8 + j] = patch k, row j. The 3D transform runs in the reference's axis
+// order (rows of each column, columns of each row, then along the group; the
+// inverse in the same order), with 8x8 transposes through shared memory.
+
+namespace {
+
+constexpr int kRowStride = 9;                 // floats per transposed row
+constexpr int kTileStride = 8 * kRowStride;   // one 8x8 tile
+constexpr int kGroupStride = 8 * kTileStride + 8;  // one group's 8 tiles (+8: bank skew)
+constexpr int kGroupsPerCta = 16;
+
+// new d_l[k*8 + i] = old d_i[k*8 + l] within each group
+__device__ __forceinline__ void transpose_group(float d[64], float* buf, int sub) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) buf[k * kTileStride + i * kRowStride + sub] = d[k * 8 + i];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) d[k * 8 + i] = buf[k * kTileStride + sub * kRowStride + i];
+    __syncwarp();
+}
+
+__device__ __forceinline__ void transform_rows(float d[64], bool inverse) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        if (inverse)
+            dct8_inv(&d[k * 8]);
+        else
+            dct8_fwd(&d[k * 8]);
+    }
+}
+
+__device__ __forceinline__ void transform_group_axis(float d[64], bool inverse) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        float v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = d[k * 8 + i];
+        if (inverse)
+            dct8_inv(v);
+        else
+            dct8_fwd(v);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) d[k * 8 + i] = v[k];
+    }
+}
+
+}  // namespace
+
+__global__ void __launch_bounds__(128) bm3d_filter_kernel(const StackJob job) {
+    __shared__ float smem[kGroupsPerCta / 4 * 4 * kGroupStride];
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & 7;
+    const int group_in_cta = threadIdx.x >> 3;
+    float* buf = smem + group_in_cta * kGroupStride;
+    const int nblocks = job.nbx * job.nby;
+    const int gblock = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
+    const bool valid = gblock < nblocks;
+    const int b = valid ? gblock : nblocks - 1;
+
+    const uint4 m0 = reinterpret_cast<const uint4*>(job.match_xy + (size_t)b * 8)[0];
+    const uint4 m1 = reinterpret_cast<const uint4*>(job.match_xy + (size_t)b * 8)[1];
+    const uint32_t mxy[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+    const uint32_t zp = job.match_z[b];
+    const int pitch = job.pitch;
+
+    float d[64];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int z = (int)((zp >> (4 * k)) & 15u);
+        const float* __restrict__ f = job.slice_frame[z];
+        const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
+        const float* p = f + (size_t)my * pitch + mx + sub;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) d[k * 8 + j] = __ldg(p + (size_t)j * pitch);
+    }
+
+    transform_rows(d, false);
+    transpose_group(d, buf, sub);
+    transform_rows(d, false);
+    transpose_group(d, buf, sub);
+    transform_group_axis(d, false);
+
+    const float thr = job.thr;
+    int kept = 0;
+#pragma unroll
+    for (int i = 0; i < 64; ++i) {
+        const float t = (i == 0 && sub == 0) ? 0.0f : thr;
+        const bool keep = fabsf(d[i]) >= t;
+        kept += keep ? 1 : 0;
+        d[i] = keep ? __fmul_rn(d[i], 1.0f / 4096.0f) : 0.0f;
+    }
+    kept += __shfl_xor_sync(kFull, kept, 1);
+    kept += __shfl_xor_sync(kFull, kept, 2);
+    kept += __shfl_xor_sync(kFull, kept, 4);
+    const float w = __fdiv_rn(1.0f, (float)kept);
+
+    transform_rows(d, true);
+    transpose_group(d, buf, sub);
+    transform_rows(d, true);
+    transpose_group(d, buf, sub);
+    transform_group_axis(d, true);
+
+    if (!valid) return;
+    const float E = job.extractor;
+    const float wv = __fsub_rn(__fadd_rn(w, E), E);
+    const int dpitch = job.dst_pitch;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int z = (int)((zp >> (4 * k)) & 15u);
+        float* num = job.slice_dst[z];
+        if (num == nullptr) continue;
+        const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
+        float* pn = num + (size_t)my * dpitch + mx + sub;
+        float* pd = pn + job.dst_plane;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            atomicAdd(pn + (size_t)j * dpitch, __fsub_rn(__fmaf_rn(w, d[k * 8 + j], E), E));
+            atomicAdd(pd + (size_t)j * dpitch, wv);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) bm3d_normalize_kernel(const NormalizeJob job) {
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (x >= job.width || y >= job.height) return;
+    const size_t o = (size_t)y * job.src_pitch + x;
+    double acc = 0.0, acw = 0.0;
+    for (int i = 0; i < job.tw; ++i) {
+        acc += (double)job.num[i][o];
+        acw += (double)job.num[i][o + job.den_offset];
+    }
+    job.out[(size_t)y * job.out_pitch + x] = (float)(acc / acw);
+}
+
+// ---------------------------------------------------------------------------
+namespace {
+constexpr int kThreads = 128;  // 16 blocks (8 lanes each) per CTA
+int block_grid(const StackJob& job) { return (job.nbx * job.nby * 8 + kThreads - 1) / kThreads; }
+}  // namespace
+
+cudaError_t launch_match(const StackJob& job, cudaStream_t stream) {
+    if (job.radius < 3)
+        bm3d_match_kernel<true><<<block_grid(job), kThreads, 0, stream>>>(job);
+    else
+        bm3d_match_kernel<false><<<block_grid(job), kThreads, 0, stream>>>(job);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_filter(const StackJob& job, cudaStream_t stream) {
+    bm3d_filter_kernel<<<block_grid(job), kThreads, 0, stream>>>(job);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream) {
+    dim3 grid((job.width + 31) / 32, (job.height + 7) / 8);
+    bm3d_normalize_kernel<<<grid, 256, 0, stream>>>(job);
+    return cudaGetLastError();
+}
+
+}  // namespace vsfeel

@@ -1,0 +1,67 @@
+"""Builds the product library vsfeel/libvsfeel_bm3d.so for sm_100a.
+
+nvcc cross-compiles here without a GPU; the .so is built in-tree so that it
+travels with the repository snapshot. Device code is compiled with
+-fmad=false: the kernels spell every fused operation explicitly
+(__fmaf_rn), so no other multiply-add may be contracted.
+"""
+
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+CSRC = Path(__file__).resolve().parent
+PKG = CSRC.parent / "vsfeel"
+INCLUDE = CSRC.parent.parent / "include"
+LIB = PKG / "libvsfeel_bm3d.so"
+SOURCES = ["bm3d_kernels.cu", "bm3d_engine.cu"]
+HEADERS = ["bm3d_device.cuh"]
+
+NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
+FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-O3", "-lineinfo", "-std=c++17", "-fmad=false",
+    "-Xcompiler", "-fPIC,-O2,-fvisibility=hidden", "-I", str(INCLUDE),
+]
+
+
+def _stale() -> bool:
+    if not LIB.exists():
+        return True
+    t = LIB.stat().st_mtime
+    deps = [CSRC / s for s in SOURCES + HEADERS] + [INCLUDE / "vsfeel_bm3d.h", Path(__file__)]
+    return any(d.stat().st_mtime > t for d in deps)
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and not _stale():
+        return LIB
+    objs = []
+    build_dir = CSRC / "_build"
+    build_dir.mkdir(exist_ok=True)
+    for src in SOURCES:
+        obj = build_dir / (Path(src).stem + ".o")
+        cmd = [NVCC, *FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        proc = subprocess.run(cmd, capture_output=True, text=True)
+        if proc.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}:\n{proc.stdout}\n{proc.stderr}")
+        if verbose:
+            sys.stderr.write(proc.stderr)
+        objs.append(str(obj))
+    tmp = LIB.with_suffix(".so.tmp")
+    proc = subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a",
+                           *objs, "-o", str(tmp), "-lcudart_static", "-lrt", "-lpthread", "-ldl"],
+                          capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"link failed:\n{proc.stdout}\n{proc.stderr}")
+    os.replace(tmp, LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

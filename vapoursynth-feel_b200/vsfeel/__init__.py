@@ -1,0 +1,268 @@
+"""vsfeel (B200): BM3Dv2 basic estimate behind the reference's plugin API.
+
+``BM3Dv2(clip, ref=None, sigma=..., block_step=..., bm_range=..., radius=...,
+ps_num=..., ps_range=..., num_streams=..., extractor_exp=...)`` takes and
+returns the same arguments as ``core.vsfeel.BM3Dv2`` (README.md:44-77,
+src/bm3d.cpp:1558-1574). Clips are ``VideoNode`` objects holding float32
+planes; ``clip_from_array`` builds one from numpy arrays. Errors raise
+``vsfeel.Error`` with the reference's messages.
+
+All denoising runs in libvsfeel_bm3d.so on the GPU through the C ABI of
+include/vsfeel_bm3d.h; there is no CPU path.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Sequence
+
+import numpy as np
+
+from . import _lib
+
+__all__ = ["Error", "VideoFormat", "GRAYS", "YUV420PS", "YUV444PS", "VideoNode", "VideoFrame",
+           "clip_from_array", "BM3Dv2", "bm3d_device"]
+
+
+class Error(Exception):
+    """Raised for invalid arguments or GPU failures (mirrors vapoursynth.Error)."""
+
+
+@dataclass(frozen=True)
+class VideoFormat:
+    color_family: int
+    sample_type: int
+    bits_per_sample: int
+    subsampling_w: int
+    subsampling_h: int
+
+    @property
+    def num_planes(self) -> int:
+        return 1 if self.color_family == _lib.CF_GRAY else 3
+
+
+GRAYS = VideoFormat(_lib.CF_GRAY, _lib.ST_FLOAT, 32, 0, 0)
+YUV420PS = VideoFormat(_lib.CF_YUV, _lib.ST_FLOAT, 32, 1, 1)
+YUV444PS = VideoFormat(_lib.CF_YUV, _lib.ST_FLOAT, 32, 0, 0)
+
+
+class VideoFrame:
+    def __init__(self, planes: Sequence[np.ndarray], fmt: VideoFormat):
+        self.planes = list(planes)
+        self.format = fmt
+
+    def __getitem__(self, p: int) -> np.ndarray:
+        return self.planes[p]
+
+    @property
+    def width(self) -> int:
+        return self.planes[0].shape[1]
+
+    @property
+    def height(self) -> int:
+        return self.planes[0].shape[0]
+
+
+class VideoNode:
+    """A clip of ``num_frames`` frames; plane p is an array (N, h_p, w_p)."""
+
+    def __init__(self, planes: Sequence[np.ndarray], fmt: VideoFormat):
+        self._planes = list(planes)
+        self.format = fmt
+        self.num_frames = int(self._planes[0].shape[0])
+        self.height = int(self._planes[0].shape[1])
+        self.width = int(self._planes[0].shape[2])
+
+    def get_frame(self, n: int) -> VideoFrame:
+        if not 0 <= n < self.num_frames:
+            raise Error("frame index out of range")
+        return VideoFrame([p[n] for p in self._planes], self.format)
+
+    def plane_array(self, p: int = 0) -> np.ndarray:
+        return self._planes[p]
+
+    def video_info(self) -> _lib.VideoInfo:
+        f = self.format
+        return _lib.VideoInfo(self.width, self.height, self.num_frames, f.color_family,
+                              f.sample_type, f.bits_per_sample, f.subsampling_w, f.subsampling_h)
+
+
+def clip_from_array(luma: np.ndarray, u: np.ndarray | None = None, v: np.ndarray | None = None,
+                    fmt: VideoFormat | None = None) -> VideoNode:
+    """A GRAYS clip from (N, H, W) luma, or a YUV clip when u and v are given."""
+    luma = np.asarray(luma)
+    if luma.ndim == 2:
+        luma = luma[None]
+    if u is None:
+        return VideoNode([luma], fmt or GRAYS)
+    if fmt is None:
+        sw = int(round(np.log2(luma.shape[2] / u.shape[2]))) if u.shape[2] else 0
+        sh = int(round(np.log2(luma.shape[1] / u.shape[1]))) if u.shape[1] else 0
+        fmt = VideoFormat(_lib.CF_YUV, _lib.ST_FLOAT, 32, sw, sh)
+    return VideoNode([luma, np.asarray(u), np.asarray(v)], fmt)
+
+
+def _array_arg(value, name: str, cast):
+    if value is None:
+        return [], 0
+    vals = list(value) if isinstance(value, (list, tuple, np.ndarray)) else [value]
+    if len(vals) > 3:
+        raise Error(f"BM3D: \"{name}\" has more than 3 elements")
+    return [cast(v) for v in vals], len(vals)
+
+
+def _make_args(ref, sigma, block_step, bm_range, radius, ps_num, ps_range, num_streams,
+               extractor_exp) -> tuple[_lib.Args, object]:
+    a = _lib.Args()
+    for name, value, cast in (("sigma", sigma, float), ("block_step", block_step, int),
+                              ("bm_range", bm_range, int), ("ps_num", ps_num, int),
+                              ("ps_range", ps_range, int)):
+        vals, n = _array_arg(value, name, cast)
+        arr = getattr(a, name)
+        for i, v in enumerate(vals):
+            arr[i] = v
+        setattr(a, f"{name}_count", n)
+    for name, value in (("radius", radius), ("num_streams", num_streams),
+                        ("extractor_exp", extractor_exp)):
+        if value is not None:
+            setattr(a, name, int(value))
+            setattr(a, f"{name}_set", 1)
+    keep = None
+    if ref is not None:
+        keep = ref.video_info()
+        a.has_ref = 1
+        a.ref_info = ctypes.pointer(keep)
+    return a, keep
+
+
+class _Context:
+    """Owns one vsfeel_bm3d context."""
+
+    def __init__(self, clip: VideoNode, args: _lib.Args, device: int):
+        self.lib = _lib.load()
+        self.vi = clip.video_info()
+        h = ctypes.c_void_p()
+        rc = self.lib.vsfeel_bm3d_create(ctypes.byref(args), ctypes.byref(self.vi), device,
+                                         ctypes.byref(h))
+        if rc != _lib.OK:
+            raise Error(_lib.last_error(self.lib))
+        self.handle = h
+
+    def check(self, rc: int) -> None:
+        if rc != _lib.OK:
+            raise Error(_lib.last_error(self.lib))
+
+    def info(self) -> _lib.Info:
+        inf = _lib.Info()
+        self.check(self.lib.vsfeel_bm3d_get_info(self.handle, ctypes.byref(inf)))
+        return inf
+
+    def __del__(self):
+        h = getattr(self, "handle", None)
+        if h:
+            self.lib.vsfeel_bm3d_free(h)
+            self.handle = None
+
+
+class BM3DNode(VideoNode):
+    """The filter's output clip. Frames are denoised on demand (``get_frame``,
+    the VapourSynth request path) or all at once (``output``)."""
+
+    def __init__(self, clip: VideoNode, ctx: _Context):
+        super().__init__([clip.plane_array(p) for p in range(clip.format.num_planes)], clip.format)
+        self._src = clip
+        self._ctx = ctx
+        self._luma_src = np.ascontiguousarray(clip.plane_array(0), dtype=np.float32)
+
+    @property
+    def info(self) -> _lib.Info:
+        return self._ctx.info()
+
+    def frame_range(self, n: int) -> tuple[int, int]:
+        lo, hi = ctypes.c_int(), ctypes.c_int()
+        self._ctx.check(self._ctx.lib.vsfeel_bm3d_frame_range(self._ctx.handle, n,
+                                                               ctypes.byref(lo), ctypes.byref(hi)))
+        return lo.value, hi.value
+
+    def get_frame(self, n: int) -> VideoFrame:
+        if not 0 <= n < self.num_frames:
+            raise Error("frame index out of range")
+        src = self._luma_src
+        out = np.empty((self.height, self.width), dtype=np.float32)
+
+        @_lib.FETCH_FN
+        def fetch(user, f, stride):
+            stride[0] = src.strides[1]
+            return src[f].ctypes.data
+
+        @_lib.RELEASE_FN
+        def release(user, f):
+            pass
+
+        self._ctx.check(self._ctx.lib.vsfeel_bm3d_get_frame(
+            self._ctx.handle, n, fetch, release, None, out.ctypes.data, out.strides[0]))
+        planes = [out] + [self._src.plane_array(p)[n] for p in range(1, self.format.num_planes)]
+        return VideoFrame(planes, self.format)
+
+    def output(self, first: int = 0, count: int | None = None,
+               out: np.ndarray | None = None) -> np.ndarray:
+        """Denoised luma of frames first..first+count-1 as (count, H, W)."""
+        count = self.num_frames - first if count is None else count
+        if out is None:
+            out = np.empty((count, self.height, self.width), dtype=np.float32)
+        src = self._luma_src
+        self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_host(
+            self._ctx.handle, src.ctypes.data, src.strides[0], src.strides[1], out.ctypes.data,
+            out.strides[0], out.strides[1], first, count))
+        return out
+
+
+def BM3Dv2(clip: VideoNode, ref: VideoNode | None = None, sigma=None, block_step=None,
+           bm_range=None, radius=None, ps_num=None, ps_range=None, num_streams=None,
+           extractor_exp=None, device: int = 0) -> BM3DNode:
+    """core.vsfeel.BM3Dv2: the BM3D basic estimate (hard thresholding)."""
+    if not isinstance(clip, VideoNode):
+        clip = clip_from_array(np.asarray(clip))
+    args, keep = _make_args(ref, sigma, block_step, bm_range, radius, ps_num, ps_range,
+                            num_streams, extractor_exp)
+    ctx = _Context(clip, args, device)
+    del keep
+    return BM3DNode(clip, ctx)
+
+
+def bm3d_device(frames, sigma=None, block_step=None, bm_range=None, radius=None, ps_num=None,
+                ps_range=None, extractor_exp=None, out=None):
+    """Denoises a CUDA float32 tensor (N, H, W) in place on torch's current
+    stream and returns the output tensor (N, H, W)."""
+    import torch
+
+    if not (isinstance(frames, torch.Tensor) and frames.is_cuda and frames.dtype == torch.float32):
+        raise Error("BM3D: frames must be a CUDA float32 tensor")
+    if frames.dim() != 3 or frames.stride(2) != 1:
+        raise Error("BM3D: frames must be (N, H, W) with contiguous rows")
+    n, h, w = frames.shape
+    fmt = GRAYS
+    vi = _lib.VideoInfo(w, h, n, fmt.color_family, fmt.sample_type, 32, 0, 0)
+    args, _ = _make_args(None, sigma, block_step, bm_range, radius, ps_num, ps_range, None,
+                         extractor_exp)
+    lib = _lib.load()
+    handle = ctypes.c_void_p()
+    if lib.vsfeel_bm3d_create(ctypes.byref(args), ctypes.byref(vi), frames.device.index or 0,
+                              ctypes.byref(handle)) != _lib.OK:
+        raise Error(_lib.last_error(lib))
+    try:
+        if out is None:
+            out = torch.empty((n, h, w), dtype=torch.float32, device=frames.device)
+        stream = torch.cuda.current_stream(frames.device).cuda_stream
+        rc = lib.vsfeel_bm3d_process_device(handle, frames.data_ptr(), frames.stride(0),
+                                            frames.stride(1), out.data_ptr(), out.stride(0),
+                                            out.stride(1), 0, n, stream)
+        if rc != _lib.OK:
+            raise Error(_lib.last_error(lib))
+        # the context's scratch buffers are freed by vsfeel_bm3d_free, which
+        # waits for its own stream only: finish this stream first
+        torch.cuda.current_stream(frames.device).synchronize()
+    finally:
+        lib.vsfeel_bm3d_free(handle)
+    return out
