@@ -1,0 +1,350 @@
+#!/usr/bin/env python
+"""Benchmark of the BM3Dv2 basic estimate on B200.
+
+Workload (one step): denoise a seeded synthetic YUV420PS clip, 1920x1080,
+32 frames, radius 2, sigma 3, block_step 4, bm_range 16, ps_num 2,
+ps_range 7, extractor_exp 0 (luma denoised, chroma passed through), the
+reference benchmark's BM3D settings (benchmark/bench.py:108-121,167-180).
+
+* value -- Mpx/s with the clip already in HBM (process_device), timed with
+  CUDA events on the launch stream; the inputs (265 MB) exceed L2.
+* e2e -- the same metric through the plugin-facing host call
+  (vsfeel_bm3d_process_host) from pinned host memory, host->device and
+  device->host copies of every frame inside the timed region.
+* roofline -- the dominant kernel (block matching) timed live with CUDA
+  events: algorithmic bytes per launch (8 B/px x one frame) / launch time.
+* cpu_baseline -- the oracle (C++ restatement of the reference) on the host
+  cores, on a bounded sample of whole stacks of the same workload.
+
+``--impl reference`` times the reference's own shaders compiled for the CPU
+(oracle/_ref) on the same workload instead; N>1 ranks other than 0 exit.
+
+Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+For N > 1 launch one process per GPU with torch.distributed.run; every rank
+denoises its own clip (weak scaling, no collective on the data path).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+PKG = ROOT / "vapoursynth-feel_b200"
+for _p in (str(ROOT), str(PKG)):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "BM3Dv2 1080p Mpx/s: plain vs batched vs fwd+bwd at ≤1e-4 max abs err"
+UNIT = "Mpx/s"
+WIDTH, HEIGHT, FRAMES = 1920, 1080, 32
+PARAMS = dict(sigma=3.0, block_step=4, bm_range=16, radius=2, ps_num=2, ps_range=7,
+              extractor_exp=0)
+CONFIG = {
+    "workload": "bm3dv2_plain_yuv420ps_1920x1080x32_r2",
+    "format": "YUV420PS (luma denoised, 960x540 chroma passed through)",
+    "width": WIDTH, "height": HEIGHT, "frames_per_step": FRAMES, **PARAMS,
+    "noise_sigma_255": 3.0, "translation_px": 4,
+    "l2": "inputs (265 MB of luma) larger than L2 (126 MB); no flush",
+}
+BYTES_PER_PX = 8  # algorithmic: read 4 + write 4 of luma per output pixel
+PROFILE_FILE = ROOT / "profiles" / "bm3d_match_kernel__1080p_r2.txt"
+
+
+def _peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def _profile_traffic():
+    """dram bytes per launch of the match kernel from the committed ncu summary."""
+    try:
+        for line in PROFILE_FILE.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch_full_size:"):
+                return int(float(line.split(":", 1)[1].split()[0]))
+    except Exception:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_id: str):
+        self.device_id = device_id
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.device_id, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=10)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, sm_max, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                sm_max = max(sm_max, float(f[1]))
+            except ValueError:
+                continue
+            for name, val in zip(names, f[4:8]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": sm_max,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def _device_id(torch, dev) -> str:
+    try:
+        u = str(torch.cuda.get_device_properties(dev).uuid)
+        return u if u.startswith("GPU-") else f"GPU-{u}"
+    except Exception:
+        return str(dev)
+
+
+def cpu_baseline_port(luma):
+    """The oracle (C++ restatement of the reference) on the host cores: whole
+    stacks of the workload until about 10 s have passed (at most 16)."""
+    from oracle import Oracle, Params
+
+    o = Oracle()
+    p = Params(**PARAMS)
+    threads = os.cpu_count() or 1
+    done, t0 = 0, time.perf_counter()
+    while done < 16:
+        o.stack(luma, p, (luma.shape[0] // 2 + done) % luma.shape[0], nthreads=threads)
+        done += 1
+        if time.perf_counter() - t0 > 10.0:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": done * WIDTH * HEIGHT / dt / 1e6, "unit": UNIT, "cores": threads,
+            "kind": "port",
+            "sample": f"{done} stacks (one output frame each in the steady state) of the "
+                      f"1920x1080 r2 workload, oracle fp32 with {threads} threads, {dt:.1f} s"}
+
+
+def run_reference(args) -> int:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import Oracle, Params, ReferenceShaders
+    from vsfeel.synthetic import make_clip
+
+    luma = make_clip(5, HEIGHT, WIDTH, sigma=3.0, shift=4, seed=2000)
+    p = Params(**PARAMS)
+    threads = os.cpu_count() or 1
+    nby = (HEIGHT - 9 + 2 * p.block_step) // p.block_step
+    if ReferenceShaders.available():
+        ref = ReferenceShaders()
+        kind = "reference"
+
+        def step(rows):
+            ref.stack_rows(luma, p, 2, (nby - rows) // 2, rows, nthreads=threads)
+        what = "reference shaders (src/bm3d.comp) compiled for the CPU"
+    else:
+        o = Oracle()
+        kind = "port"
+
+        def step(rows):
+            o.stack(luma, p, 2, nthreads=threads)
+        what = "oracle restatement (reference shaders not built)"
+    # size each step so that warmup + steps take about 150 s
+    t0 = time.perf_counter()
+    step(8)
+    per_row = (time.perf_counter() - t0) / 8
+    total = args.steps + args.warmup
+    rows = int(max(4, min(nby, 150.0 / max(total, 1) / max(per_row, 1e-6))))
+    if kind == "port":
+        rows = nby
+    for _ in range(args.warmup):
+        step(rows)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step(rows)
+    dt = (time.perf_counter() - t0) / max(args.steps, 1)
+    px = rows * p.block_step * WIDTH
+    value = px / dt / 1e6
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": CONFIG,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": kind,
+                         "sample": f"{rows} block rows ({px} px of reference blocks) of stack 2 "
+                                   f"per step, {what}, {threads} threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main() -> int:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--frames", type=int, default=FRAMES,
+                    help="frames per step (default 32; smaller only for profiling runs)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import vsfeel
+    from vsfeel.synthetic import make_chroma, make_clip
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    nfr = args.frames
+    luma = make_clip(nfr, HEIGHT, WIDTH, sigma=3.0, shift=4, seed=2000 + rank)
+    u = make_chroma(nfr, HEIGHT // 2, WIDTH // 2, seed=2000 + rank)
+    v = make_chroma(nfr, HEIGHT // 2, WIDTH // 2, seed=3000 + rank)
+
+    # ---- device-resident pass ------------------------------------------------
+    node = vsfeel.BM3Dv2(vsfeel.clip_from_array(luma, u, v), device=local_rank, **PARAMS)
+    d_src = torch.from_numpy(luma).to(dev)
+    d_out = torch.empty_like(d_src)
+    for _ in range(args.warmup):
+        node.output_device(d_src, d_out)
+    torch.cuda.synchronize()
+    barrier()
+    clocks = ClockSampler(_device_id(torch, dev))
+    clocks.start()
+    time.sleep(0.3)
+    node.trace(True)
+    launches0 = node.launch_count()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    start.record()
+    for _ in range(args.steps):
+        node.output_device(d_src, d_out)
+    stop.record()
+    torch.cuda.synchronize()
+    elapsed_ms = start.elapsed_time(stop)
+    launches = node.launch_count() - launches0
+    kt = node.trace_read()
+    node.trace(False)
+    clk = clocks.stop()
+    barrier()
+    elapsed_ms = max_over_ranks(elapsed_ms)
+    ms_per_step = elapsed_ms / args.steps
+    px_per_step = nfr * WIDTH * HEIGHT
+    value = world * px_per_step / (ms_per_step / 1e3) / 1e6
+
+    # ---- end to end through the host entry point (pinned buffers) -----------
+    e2e = None
+    if not args.no_e2e:
+        h_src = torch.from_numpy(luma).pin_memory()
+        h_out = torch.empty(luma.shape, dtype=torch.float32).pin_memory()
+        enode = vsfeel.BM3Dv2(vsfeel.clip_from_array(h_src.numpy(), u, v), device=local_rank,
+                              **PARAMS)
+        out_np = h_out.numpy()
+        for _ in range(max(1, args.warmup)):
+            enode.output(out=out_np)
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            enode.output(out=out_np)
+        e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
+        e2e = {"value": world * px_per_step / e2e_s / 1e6, "unit": UNIT,
+               "h2d_bytes_per_step": int(h_src.numel() * 4),
+               "d2h_bytes_per_step": int(h_out.numel() * 4),
+               "max_abs_diff_vs_device_path": float(np.abs(out_np - d_out.cpu().numpy()).max())}
+
+    # ---- roofline of the dominant kernel ------------------------------------
+    match_ms, match_n = kt["bm3d_match_kernel"]
+    avg_s = match_ms / max(match_n, 1) / 1e3
+    alg_bytes = BYTES_PER_PX * WIDTH * HEIGHT
+    achieved = alg_bytes / avg_s / 1e9 if avg_s > 0 else 0.0
+    peak, peak_src = _peaks()
+    traffic = _profile_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic,
+                "kernel": "bm3d_match_kernel", "peak_source": peak_src,
+                "avg_launch_ms": avg_s * 1e3, "algorithmic_bytes_per_launch": alg_bytes,
+                "kernel_ms_share": {k: round(ms / max(sum(x[0] for x in kt.values()), 1e-9), 4)
+                                    for k, (ms, _) in kt.items()}}
+
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {**CONFIG, "frames_per_step": nfr,
+                   "parallelism": f"frame-shard x{world} (independent clips)"},
+        "e2e": e2e,
+        "gpu_launches": int(launches),
+        "roofline": roofline,
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_port(luma)
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -117,8 +117,9 @@ VSFEEL_API int vsfeel_bm3d_process_host(vsfeel_bm3d* ctx, const float* src, ptrd
                              int first, int count);
 
 /* Whole clip already in device memory (strides in floats), enqueued on
- * `stream` (a cudaStream_t; NULL = the context's own stream). Returns after
- * the work is enqueued; synchronise the stream before reading dst. */
+ * `stream` (a cudaStream_t, used as given: NULL is the default stream).
+ * Returns after the work is enqueued; synchronise the stream before reading
+ * dst, and keep src and dst alive until then. */
 VSFEEL_API int vsfeel_bm3d_process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
                                int64_t src_row_stride, float* dst, int64_t dst_frame_stride,
                                int64_t dst_row_stride, int first, int count, void* stream);
@@ -143,6 +144,18 @@ VSFEEL_API int vsfeel_bm3d_match_table_device(vsfeel_bm3d* ctx, const float* src
 
 /* Kernel launches issued by this context since creation (all kernels). */
 VSFEEL_API int64_t vsfeel_bm3d_launch_count(const vsfeel_bm3d* ctx);
+
+/* Per-kernel GPU timing with CUDA events on the launch stream (the
+ * reference's BM3D_GPUTRACE, src/bm3d.cpp:978-994). enable != 0 starts (and
+ * resets) the trace, 0 stops it. */
+enum { VSFEEL_KERNEL_MATCH = 0, VSFEEL_KERNEL_FILTER = 1, VSFEEL_KERNEL_NORMALIZE = 2,
+       VSFEEL_KERNEL_KINDS = 3 };
+VSFEEL_API int vsfeel_bm3d_trace(vsfeel_bm3d* ctx, int enable);
+
+/* Waits for the traced work, then returns per kernel kind the summed device
+ * milliseconds and the number of traced launches. */
+VSFEEL_API int vsfeel_bm3d_trace_read(vsfeel_bm3d* ctx, double ms[VSFEEL_KERNEL_KINDS],
+                                      int64_t launches[VSFEEL_KERNEL_KINDS]);
 
 /* The calling thread's last error message ("" when none). */
 VSFEEL_API const char* vsfeel_bm3d_last_error(void);

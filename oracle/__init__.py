@@ -164,7 +164,23 @@ class ReferenceShaders:
         lib.ref_bm3d_clip.restype = _i
         lib.ref_bm3d_stack.argtypes = [_p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i, _i, _i, _p]
         lib.ref_bm3d_stack.restype = _i
+        lib.ref_bm3d_stack_rows.argtypes = [_p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i, _i, _i, _i,
+                                            _i]
+        lib.ref_bm3d_stack_rows.restype = _i
         self.lib = lib
+
+    def stack_rows(self, frames, params: Params, m: int, row_first: int, row_count: int,
+                   nthreads=None) -> None:
+        """Runs stack m's estimation over block rows [row_first, row_first+row_count)
+        only (a timing sample; the result is discarded)."""
+        a = _frames(frames)
+        n, h, w = a.shape
+        p = params
+        rc = self.lib.ref_bm3d_stack_rows(_ptr(a), n, w, h, _f(p.sigma), p.block_step, p.bm_range,
+                                          p.radius, p.ps_num, p.ps_range, p.extractor_exp, m,
+                                          row_first, row_count, nthreads or _default_threads())
+        if rc != 0:
+            raise ValueError("reference harness rejected the arguments")
 
     @classmethod
     def available(cls) -> bool:

@@ -200,8 +200,11 @@ bool setup(Setup& S, int nframes, int W, int H, float sigma, int step, int R, in
     return true;
 }
 
-// One stack: zero-fill, then the estimation dispatch (src/bm3d.cpp:558-601).
-void run_stack(const Setup& S, float* res, float* src, int m, size_t res_off, int nthreads) {
+// One stack: zero-fill, then the estimation dispatch (src/bm3d.cpp:558-601),
+// restricted to workgroup rows [gy_first, gy_first + gy_count) when gy_count
+// is not negative (a timing sample of the dispatch).
+void run_stack(const Setup& S, float* res, float* src, int m, size_t res_off, int nthreads,
+               int gy_first = 0, int gy_count = -1) {
     std::memset(res + res_off, 0, sizeof(float) * S.tw * 2 * S.pe);
     ref_bm3d_bind(0, res);
     ref_bm3d_bind(1, src);
@@ -210,7 +213,28 @@ void run_stack(const Setup& S, float* res, float* src, int m, size_t res_off, in
     const uint32_t ls[3] = {32, 1, 1};
     const int gx = (S.W + 4 * S.step - 1) / (4 * S.step);
     const int gy = (S.H + S.step - 1) / S.step;
-    dispatch(&ref_bm3d_entry, ls, gx, gy, nthreads);
+    if (gy_count < 0) {
+        dispatch(&ref_bm3d_entry, ls, gx, gy, nthreads);
+        return;
+    }
+    const int lo = std::min(std::max(gy_first, 0), gy);
+    const int hi = std::min(lo + gy_count, gy);
+    std::atomic<int> next{lo};
+    auto worker = [&]() {
+        for (;;) {
+            const int y = next.fetch_add(1);
+            if (y >= hi) break;
+            for (int x = 0; x < gx; ++x) {
+                const uint32_t gid[3] = {(uint32_t)x, (uint32_t)y, 0};
+                simt::run_workgroup(&ref_bm3d_entry, ls, gid);
+            }
+        }
+    };
+    const int nt = std::max(1, std::min(nthreads, hi - lo));
+    std::vector<std::thread> th;
+    for (int t = 1; t < nt; ++t) th.emplace_back(worker);
+    worker();
+    for (auto& t : th) t.join();
 }
 
 std::vector<float> load_frames(const Setup& S, const float* frames) {
@@ -277,6 +301,21 @@ int ref_bm3d_stack(const float* frames, int nframes, int W, int H, float sigma, 
         for (int y = 0; y < H; ++y)
             std::memcpy(slices + ((size_t)p * H + y) * W, &res[(size_t)p * S.pe + (size_t)y * S.stride],
                         sizeof(float) * W);
+    return 0;
+}
+
+// Timing sample: the estimation dispatch of stack m over workgroup rows
+// [gy_first, gy_first + gy_count) only (gy = block row, block_step pixels
+// apart). The slices are discarded. Returns 0 or -1.
+int ref_bm3d_stack_rows(const float* frames, int nframes, int W, int H, float sigma, int step, int R,
+                        int r, int P, int Q, int extractor_exp, int m, int gy_first, int gy_count,
+                        int nthreads) {
+    Setup S;
+    if (!setup(S, nframes, W, H, sigma, step, R, r, P, Q, extractor_exp)) return -1;
+    if (m < 0 || m >= nframes || gy_count < 0) return -1;
+    std::vector<float> src = load_frames(S, frames);
+    std::vector<float> res((size_t)S.tw * 2 * S.pe, 0.0f);
+    run_stack(S, res.data(), src.data(), m, 0, nthreads, gy_first, gy_count);
     return 0;
 }
 

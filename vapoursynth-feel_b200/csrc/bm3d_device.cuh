@@ -47,6 +47,7 @@ struct NormalizeJob {
 // Host-side launchers (defined beside the kernels). Each returns the launch
 // status and enqueues on `stream`.
 cudaError_t launch_match(const StackJob& job, cudaStream_t stream);
+cudaError_t launch_match_sliding(const StackJob& job, cudaStream_t stream);
 cudaError_t launch_filter(const StackJob& job, cudaStream_t stream);
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream);
 

@@ -257,6 +257,38 @@ struct vsfeel_bm3d {
     std::map<int, int> frame_slot;  // frame cache of the per-frame path
     std::vector<int> slot_frame;
 
+    // event trace: (kind, start, stop) per traced launch
+    struct Mark {
+        int kind;
+        cudaEvent_t start, stop;
+    };
+    bool tracing = false;
+    std::vector<Mark> marks;
+    std::vector<cudaEvent_t> event_pool;
+    size_t events_used = 0;
+
+    cudaEvent_t next_event() {
+        if (events_used == event_pool.size()) {
+            cudaEvent_t e;
+            VSF_CUDA(cudaEventCreate(&e));
+            event_pool.push_back(e);
+        }
+        return event_pool[events_used++];
+    }
+    // records `launch` between two events when tracing
+    template <class F>
+    void traced(int kind, cudaStream_t st, F&& launch) {
+        if (!tracing) {
+            VSF_CUDA(launch());
+            return;
+        }
+        Mark mk{kind, next_event(), next_event()};
+        VSF_CUDA(cudaEventRecord(mk.start, st));
+        VSF_CUDA(launch());
+        VSF_CUDA(cudaEventRecord(mk.stop, st));
+        marks.push_back(mk);
+    }
+
     int tw() const { return 2 * s.radius + 1; }
     int clampf(int f) const { return clampi(f, 0, s.nframes - 1); }
 
@@ -301,8 +333,8 @@ struct vsfeel_bm3d {
         job.extractor = s.extractor;
         job.match_xy = match_xy.p;
         job.match_z = match_z.p;
-        VSF_CUDA(launch_match(job, st));
-        VSF_CUDA(launch_filter(job, st));
+        traced(VSFEEL_KERNEL_MATCH, st, [&] { return launch_match(job, st); });
+        traced(VSFEEL_KERNEL_FILTER, st, [&] { return launch_filter(job, st); });
         launches += 2;
     }
 
@@ -320,7 +352,7 @@ struct vsfeel_bm3d {
         job.src_pitch = acc_pitch;
         job.out_pitch = out_pitch;
         job.out = out;
-        VSF_CUDA(vsfeel::launch_normalize(job, st));
+        traced(VSFEEL_KERNEL_NORMALIZE, st, [&] { return vsfeel::launch_normalize(job, st); });
         launches += 1;
     }
 
@@ -434,6 +466,7 @@ void vsfeel_bm3d_free(vsfeel_bm3d* ctx) {
         ctx->match_z.release();
         ctx->frames.release();
         ctx->outbuf.release();
+        for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     }
     delete ctx;
 }
@@ -471,6 +504,46 @@ int vsfeel_bm3d_get_info(const vsfeel_bm3d* ctx, vsfeel_bm3d_info* info) {
 
 int64_t vsfeel_bm3d_launch_count(const vsfeel_bm3d* ctx) { return ctx ? ctx->launches.load() : 0; }
 
+int vsfeel_bm3d_trace(vsfeel_bm3d* ctx, int enable) {
+    return guarded(ctx, [&]() -> int {
+        ctx->tracing = enable != 0;
+        ctx->marks.clear();
+        ctx->events_used = 0;
+        return VSFEEL_OK;
+    });
+}
+
+int vsfeel_bm3d_trace_read(vsfeel_bm3d* ctx, double ms[VSFEEL_KERNEL_KINDS],
+                           int64_t launches[VSFEEL_KERNEL_KINDS]) {
+    return guarded(ctx, [&]() -> int {
+        if (!ms || !launches) return fail(VSFEEL_E_ARG, "null argument");
+        for (int k = 0; k < VSFEEL_KERNEL_KINDS; ++k) {
+            ms[k] = 0.0;
+            launches[k] = 0;
+        }
+        for (const auto& mk : ctx->marks) {
+            // bounded wait for the stop event, then read the pair
+            const auto t0 = std::chrono::steady_clock::now();
+            for (;;) {
+                const cudaError_t e = cudaEventQuery(mk.stop);
+                if (e == cudaSuccess) break;
+                if (e != cudaErrorNotReady) VSF_CUDA(e);
+                const auto waited = std::chrono::duration_cast<std::chrono::milliseconds>(
+                                        std::chrono::steady_clock::now() - t0)
+                                        .count();
+                if (waited >= timeout_ms())
+                    return fail(VSFEEL_E_TIMEOUT, "timed out waiting for traced kernels");
+                std::this_thread::sleep_for(std::chrono::microseconds(50));
+            }
+            float t = 0.0f;
+            VSF_CUDA(cudaEventElapsedTime(&t, mk.start, mk.stop));
+            ms[mk.kind] += t;
+            launches[mk.kind] += 1;
+        }
+        return VSFEEL_OK;
+    });
+}
+
 int vsfeel_bm3d_process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
                                int64_t src_row_stride, float* dst, int64_t dst_frame_stride,
                                int64_t dst_row_stride, int first, int count, void* stream) {
@@ -484,7 +557,7 @@ int vsfeel_bm3d_process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_f
             return fail(VSFEEL_E_ARG, "row stride smaller than the width");
         if (src_frame_stride < src_row_stride * s.height || dst_frame_stride < dst_row_stride * s.height)
             return fail(VSFEEL_E_ARG, "frame stride smaller than a plane");
-        cudaStream_t st = stream ? (cudaStream_t)stream : ctx->stream;
+        cudaStream_t st = (cudaStream_t)stream;
         ctx->run([&](int f) { return src + (size_t)f * src_frame_stride; }, (int)src_row_stride,
                  [&](int n) { return dst + (size_t)(n - first) * dst_frame_stride; },
                  (int)dst_row_stride, first, count, st);

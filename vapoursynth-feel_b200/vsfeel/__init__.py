@@ -205,6 +205,37 @@ class BM3DNode(VideoNode):
         planes = [out] + [self._src.plane_array(p)[n] for p in range(1, self.format.num_planes)]
         return VideoFrame(planes, self.format)
 
+    def output_device(self, src, out, first: int = 0, count: int | None = None) -> None:
+        """Denoises from device memory: src is a CUDA float32 tensor
+        (num_frames, H, W) holding the clip's luma, out receives frames
+        first..first+count-1 as (count, H, W). Enqueued on torch's current
+        stream; no host copies."""
+        import torch
+
+        count = self.num_frames - first if count is None else count
+        for t in (src, out):
+            if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32
+                    and t.dim() == 3 and t.stride(2) == 1):
+                raise Error("BM3D: device buffers must be CUDA float32 (N, H, W) tensors")
+        stream = torch.cuda.current_stream(src.device).cuda_stream
+        self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_device(
+            self._ctx.handle, src.data_ptr(), src.stride(0), src.stride(1), out.data_ptr(),
+            out.stride(0), out.stride(1), first, count, stream))
+
+    def launch_count(self) -> int:
+        return int(self._ctx.lib.vsfeel_bm3d_launch_count(self._ctx.handle))
+
+    def trace(self, enable: bool) -> None:
+        """Per-kernel CUDA-event timing of the launches that follow."""
+        self._ctx.check(self._ctx.lib.vsfeel_bm3d_trace(self._ctx.handle, 1 if enable else 0))
+
+    def trace_read(self) -> dict[str, tuple[float, int]]:
+        """{kernel name: (summed device ms, launches)} of the traced launches."""
+        ms = (ctypes.c_double * _lib.KERNEL_KINDS)()
+        n = (ctypes.c_int64 * _lib.KERNEL_KINDS)()
+        self._ctx.check(self._ctx.lib.vsfeel_bm3d_trace_read(self._ctx.handle, ms, n))
+        return {name: (ms[k], n[k]) for k, name in enumerate(_lib.KERNEL_NAMES)}
+
     def output(self, first: int = 0, count: int | None = None,
                out: np.ndarray | None = None) -> np.ndarray:
         """Denoised luma of frames first..first+count-1 as (count, H, W)."""

@@ -26,6 +26,8 @@ EXPORTS = (
     "vsfeel_bm3d_get_info",
     "vsfeel_bm3d_match_table_device",
     "vsfeel_bm3d_launch_count",
+    "vsfeel_bm3d_trace",
+    "vsfeel_bm3d_trace_read",
     "vsfeel_bm3d_last_error",
     "vsfeel_bm3d_abi_version",
 )
@@ -40,6 +42,12 @@ E_MEMORY = -4
 E_TIMEOUT = -5
 E_FETCH = -6
 E_UNSUPPORTED = -7
+
+KERNEL_MATCH = 0
+KERNEL_FILTER = 1
+KERNEL_NORMALIZE = 2
+KERNEL_KINDS = 3
+KERNEL_NAMES = ("bm3d_match_kernel", "bm3d_filter_kernel", "bm3d_normalize_kernel")
 
 CF_GRAY = 1
 CF_YUV = 3
@@ -127,6 +135,11 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.vsfeel_bm3d_match_table_device.restype = c_int
     lib.vsfeel_bm3d_launch_count.argtypes = [c_p]
     lib.vsfeel_bm3d_launch_count.restype = c_i64
+    lib.vsfeel_bm3d_trace.argtypes = [c_p, c_int]
+    lib.vsfeel_bm3d_trace.restype = c_int
+    lib.vsfeel_bm3d_trace_read.argtypes = [c_p, ctypes.POINTER(ctypes.c_double),
+                                           ctypes.POINTER(c_i64)]
+    lib.vsfeel_bm3d_trace_read.restype = c_int
     lib.vsfeel_bm3d_last_error.argtypes = []
     lib.vsfeel_bm3d_last_error.restype = ctypes.c_char_p
     lib.vsfeel_bm3d_abi_version.argtypes = []
