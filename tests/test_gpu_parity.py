@@ -92,6 +92,23 @@ def test_random_configs_vs_oracle(seed, oracle_lib):
     assert np.array_equal(_cuda_tables(frames, p, [m])[m], oracle_lib.matches(frames, p, m))
 
 
+@pytest.mark.parametrize("kw", [
+    dict(sigma=6.0, block_step=4, bm_range=20, radius=2, ps_num=2, ps_range=7),   # wide window
+    dict(sigma=6.0, block_step=3, bm_range=8, radius=2, ps_num=8, ps_range=9),    # many windows
+    dict(sigma=6.0, block_step=8, bm_range=3, radius=1, ps_num=1, ps_range=1),    # tiny windows
+])
+def test_window_shapes_vs_oracle(kw, oracle_lib):
+    """Window sizes on both sides of the shared-memory budget of the tiled
+    matcher (larger ones take the direct-read kernel)."""
+    p = Params(**kw)
+    frames = make_clip(5, 80, 96, sigma=6.0, shift=5, seed=77)
+    for m in (0, 2, 4):
+        assert np.array_equal(_cuda_tables(frames, p, [m])[m], oracle_lib.matches(frames, p, m))
+    expected = oracle_lib.bm3d(frames, p)
+    out = _node(frames, **p.as_dict()).output()
+    assert np.abs(out.astype(np.float64) - expected).max() <= TYPICAL_TOL
+
+
 def test_plain_640x360_radius0_vs_oracle(oracle_lib):
     """Config: GRAYS 640x360, 8 frames, radius 0, sigma 3, step 8, bm_range 9."""
     p = Params(sigma=3.0, block_step=8, bm_range=9, radius=0, ps_num=2, ps_range=4)

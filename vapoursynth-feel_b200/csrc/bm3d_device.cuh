@@ -48,6 +48,7 @@ struct NormalizeJob {
 // status and enqueues on `stream`.
 cudaError_t launch_match(const StackJob& job, cudaStream_t stream);
 cudaError_t launch_match_sliding(const StackJob& job, cudaStream_t stream);
+bool match_sliding_fits(const StackJob& job);
 cudaError_t launch_filter(const StackJob& job, cudaStream_t stream);
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream);
 

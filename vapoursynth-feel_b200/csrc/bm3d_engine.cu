@@ -16,7 +16,7 @@
 //   normalised as soon as stack min(n + r, N - 1) is done, and its slot is
 //   reused by output n + 2r + 1.
 #include "bm3d_device.cuh"
-#include "../../include/vsfeel_bm3d.h"
+#include "vsfeel_bm3d.h"
 
 #include <algorithm>
 #include <atomic>

@@ -409,8 +409,12 @@ int block_grid(const StackJob& job) { return (job.nbx * job.nby * 8 + kThreads -
 }  // namespace
 
 cudaError_t launch_match(const StackJob& job, cudaStream_t stream) {
-    if (job.radius < 3) return launch_match_sliding(job, stream);
-    bm3d_match_kernel<false><<<block_grid(job), kThreads, 0, stream>>>(job);
+    if (job.radius < 3) {
+        if (match_sliding_fits(job)) return launch_match_sliding(job, stream);
+        bm3d_match_kernel<true><<<block_grid(job), kThreads, 0, stream>>>(job);
+    } else {
+        bm3d_match_kernel<false><<<block_grid(job), kThreads, 0, stream>>>(job);
+    }
     return cudaGetLastError();
 }
 

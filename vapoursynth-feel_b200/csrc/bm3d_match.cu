@@ -1,28 +1,30 @@
 // Block matching for radius < 3: the reference's sliding column scan
 // (src/bm3d.comp:479-538 spatial, 540-637 temporal), restructured for sm_100a.
 //
-// A CTA owns a tile of 8x4 reference blocks, 8 lanes per block. For each
-// search phase (the spatial window in frame m, then one temporal step per
-// frame) the CTA stages the frame region that every window of the tile can
-// reach (tile +- bm_range + t*ps_range) in shared memory once, and all 32
-// blocks search it from there.
+// A CTA owns a tile of 8x4 reference blocks, 8 lanes per block; a warp holds
+// four blocks of one block row, two block columns apart. For each search
+// phase (the spatial window in frame m, then one temporal step per frame) the
+// CTA stages the frame region that every window of the tile can reach
+// (tile +- bm_range + t*ps_range) in shared memory once, column-major.
 //
-// Within a block, lane s takes a chunk of K consecutive candidate rows of a
-// window and sweeps the window's columns left to right. One step loads the
-// K+7 source values of column X, updates the K column sums
+// Scan. Within a block, lane s takes a chunk of K consecutive candidate rows
+// of a window and sweeps the window's columns left to right. One step loads
+// the K+7 source values of column X (consecutive words), updates the K
+// column sums
 //     V(X) = SSD(source column X, block column min(X - left, 7))
 // and advances, per row, the reduction tree of the reference in incremental
 // form: P(j) = V(j) + V(j+1), Q(j) = P(j) + P(j+2), E(j) = Q(j) + Q(j+4) --
 // the same additions on the same operands as
 // ((c0+c1)+(c2+c3))+((c4+c5)+(c6+c7)), so every candidate error carries the
-// reference's bits.
+// reference's bits. Every error is stored to the block's error table in
+// shared memory; the lane also keeps each row's two smallest errors.
 //
-// Ranking: candidates are 64-bit keys (error bits, scan index). The error is
-// a non-negative float, so integer order is (error, index) order, and the 8
-// smallest keys are exactly the reference's merged top-8 (per-lane strict
-// insertion in index order + merge by (error, index)). Each lane keeps its 8
-// smallest keys; a candidate is offered only if it beats the smallest 8th key
-// among the block's 8 lanes, refreshed every 4 steps, so insertions are rare.
+// Selection. The reference keeps per-lane sorted top-8 lists and merges them
+// by (error, scan index); the result is the 8 smallest (error, index) keys.
+// Here the block's 8 lanes bound the 8th smallest error by the 8th smallest
+// of the window rows' two smallest errors, collect the few candidates at or
+// below the bound from the table, and place each by counting the collected
+// keys below it. The scan itself carries no branches or votes.
 #include "bm3d_device.cuh"
 
 #include <algorithm>
@@ -31,89 +33,35 @@ namespace vsfeel {
 
 namespace {
 
+constexpr unsigned kFull = 0xffffffffu;
 constexpr int kTileBX = 8, kTileBY = 4;
-constexpr int kMatchThreads = kTileBX * kTileBY * 8;  // 256
-constexpr int kMaxK = 5;
+constexpr int kGroups = kTileBX * kTileBY;
+constexpr int kMatchThreads = kGroups * 8;  // 256
+constexpr int kMinK = 2, kMaxK = 5;
+constexpr int kCollect = 64;                // candidates a block collects per pass
 constexpr uint64_t kKeyMax = (uint64_t(0x7f7fffffu) << 32) | 0x7fffffffu;  // (FLT_MAX, INT_MAX)
 
-__device__ __forceinline__ uint64_t cand_key(float err, int seq) {
-    return err < kFltMax ? ((uint64_t(__float_as_uint(err)) << 32) | uint32_t(seq)) : kKeyMax;
+__device__ __forceinline__ uint64_t make_key(float err, int seq) {
+    return (uint64_t(__float_as_uint(err)) << 32) | uint32_t(seq);
 }
 
 __device__ __forceinline__ float key_err(uint64_t k) { return __uint_as_float(uint32_t(k >> 32)); }
 
-__device__ __forceinline__ uint64_t umin64(uint64_t a, uint64_t b) { return a < b ? a : b; }
-
-struct KeyList {
-    uint64_t k[8];  // ascending
-
-    __device__ __forceinline__ void reset() {
+__device__ __forceinline__ int warp_max(int v) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) k[i] = kKeyMax;
-    }
-    // keys are distinct, so `<` places c exactly
-    __device__ __forceinline__ void insert(uint64_t c) {
-#pragma unroll
-        for (int i = 7; i > 0; --i) {
-            const bool sh = c < k[i - 1];
-            const bool pl = c < k[i];
-            k[i] = sh ? k[i - 1] : (pl ? c : k[i]);
-        }
-        k[0] = c < k[0] ? c : k[0];
-    }
-};
-
-__device__ __forceinline__ uint64_t group_min(uint64_t v, unsigned gmask) {
-#pragma unroll
-    for (int off = 1; off < 8; off <<= 1) v = umin64(v, __shfl_xor_sync(gmask, v, off));
+    for (int off = 1; off < 32; off <<= 1) v = max(v, __shfl_xor_sync(kFull, v, off));
     return v;
-}
-
-__device__ __forceinline__ int group_max(int v, unsigned gmask) {
-#pragma unroll
-    for (int off = 1; off < 8; off <<= 1) v = max(v, __shfl_xor_sync(gmask, v, off));
-    return v;
-}
-
-// The `count` smallest keys of the group's 8 lane lists, in order; every
-// lane of the group receives them. Equal keys (sentinels) resolve to the
-// lower lane.
-template <int kCount>
-__device__ __forceinline__ void merge_keys(KeyList L, uint64_t out[8], int count, unsigned gmask) {
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int q = 0; q < kCount; ++q) {
-        if (q >= count) {
-            out[q] = kKeyMax;
-            continue;
-        }
-        uint64_t best = L.k[0];
-        int src = lane;
-#pragma unroll
-        for (int off = 1; off < 8; off <<= 1) {
-            const uint64_t o = __shfl_xor_sync(gmask, best, off);
-            const int os = __shfl_xor_sync(gmask, src, off);
-            const bool take = o < best || (o == best && os < src);
-            best = take ? o : best;
-            src = take ? os : src;
-        }
-        out[q] = best;
-        if (lane == src) {
-#pragma unroll
-            for (int i = 0; i < 7; ++i) L.k[i] = L.k[i + 1];
-            L.k[7] = kKeyMax;
-        }
-    }
 }
 
 // A search window: candidate columns left..left+rw-1, rows top..top+h-1,
-// scan indices seq_base + (cy-top)*rw + (cx-left).
+// scan indices seq_base + (cy-top)*rw + (cx-left); its errors sit in the
+// block's table at eoff + (cx-left)*h + (cy-top).
 struct Window {
-    int left, top, rw, h, seq_base;
+    int left, top, rw, h, seq_base, eoff;
 };
 
 __device__ __forceinline__ Window make_window(int cx, int cy, int range, int width, int height,
-                                              int seq_base) {
+                                              int seq_base, int eoff) {
     Window w;
     w.left = max(cx - range, 0);
     const int right = min(cx + range, width - 8);
@@ -122,25 +70,18 @@ __device__ __forceinline__ Window make_window(int cx, int cy, int range, int wid
     w.rw = right - w.left + 1;
     w.h = bottom - w.top + 1;
     w.seq_base = seq_base;
+    w.eoff = eoff;
     return w;
 }
 
-// Source of a phase: the staged region in shared memory (kSmem) or the frame
-// in global memory.
-struct Source {
-    const float* smem;  // region origin (rx0, ry0), row stride ss
-    int rx0, ry0, ss;
-    const float* __restrict__ frame;
-    int pitch;
+// The staged region, column-major with column stride cs (odd), so the K+7
+// source rows a lane needs at one column are consecutive words.
+struct Region {
+    const float* smem;
+    int rx0, ry0, cs;
 };
 
-template <bool kSmem>
-__device__ __forceinline__ float src_at(const Source& s, int row, int col) {
-    if (kSmem) return s.smem[(row - s.ry0) * s.ss + (col - s.rx0)];
-    return __ldg(s.frame + (size_t)row * s.pitch + col);
-}
-
-// SSD of one column of the block (bc, 8 values) against w[q..q+7].
+// SSD of one column of the block (bc) against w[q..q+7].
 template <int K>
 __device__ __forceinline__ float column_ssd_at(const float bc[8], const float w[K + 7], int q) {
     float ev = 0.0f, od = 0.0f;
@@ -155,42 +96,45 @@ __device__ __forceinline__ float column_ssd_at(const float bc[8], const float w[
 }
 
 // One lane's chunk: rows r0..r0+nrows-1 of window `win` (nrows may be 0),
-// columns swept for `jcount` steps (uniform across the group; steps past the
-// window's own width are padding). cur_s: the block's 64 values in shared
-// memory, column-major; c7: block column 7 in registers.
-template <int K, bool kSmem>
-__device__ __forceinline__ void scan_chunk(const Source& src, const float* cur_s, const float c7[8],
+// `jcount` column steps (warp-uniform; steps past the window's width are
+// padding). cur_s: the block's 64 values in shared memory, column-major; c7:
+// block column 7 in registers. Errors go to table E; each row's two smallest
+// errors are merged into lb, this lane's 8 smallest such values (ascending).
+template <int K>
+__device__ __forceinline__ void scan_chunk(const Region& reg, const float* cur_s, const float c7[8],
                                            const Window& win, int r0, int nrows, int jcount,
-                                           int row_max, unsigned gmask, KeyList& L,
-                                           uint64_t& thr) {
+                                           float* E, float lb[8]) {
     float vp[K], pr[K][2], qr[K][4];
+    float m1[K], m2[K];
+#pragma unroll
+    for (int q = 0; q < K; ++q) m1[q] = m2[q] = kFltMax;
     const int xmax = win.left + win.rw + 6;
-    const int seq_row0 = win.seq_base + (r0 - win.top) * win.rw;
-    // shared memory: rows past row_max exist (the region is padded) and only
-    // feed masked rows; global memory: clamp them into the frame
-    const float* sbase = kSmem ? src.smem + (r0 - src.ry0) * src.ss - src.rx0 : nullptr;
-    const int ss = src.ss;
+    // rows past the window exist in each staged column (padding) and only
+    // feed masked rows
+    const float* sbase = reg.smem + (r0 - reg.ry0) - reg.rx0 * reg.cs;
+    const int cs = reg.cs;
+    float* ecol = E + win.eoff + (r0 - win.top);
 
     auto load_col = [&](int X, float w[K + 7]) {
+        const float* col = sbase + X * cs;
 #pragma unroll
-        for (int k = 0; k < K + 7; ++k) {
-            if (kSmem)
-                w[k] = sbase[k * ss + X];
-            else
-                w[k] = __ldg(src.frame + (size_t)min(r0 + k, row_max) * src.pitch + X);
-        }
+        for (int k = 0; k < K + 7; ++k) w[k] = col[k];
     };
-    auto offer = [&](float e, int q, int d) {
-        if (q < nrows && d < win.rw) {
-            const uint64_t key = cand_key(e, seq_row0 + q * win.rw + d);
-            if (key < thr) {
-                L.insert(key);
-                thr = umin64(thr, L.k[7]);
+    auto emit = [&](const float e[K], int d) {
+        if (d < win.rw) {
+            float* out = ecol + d * win.h;
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                if (q < nrows) {
+                    out[q] = e[q];
+                    m2[q] = fminf(m2[q], fmaxf(m1[q], e[q]));
+                    m1[q] = fminf(m1[q], e[q]);
+                }
             }
         }
     };
 
-    // warm-up: columns 0..7 of the block, steps j = 0..7 (candidate 0 at j = 7)
+    // warm-up: block columns 0..7, steps j = 0..7 (candidate column 0 at j = 7)
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
         float bc[8];
@@ -198,67 +142,177 @@ __device__ __forceinline__ void scan_chunk(const Source& src, const float* cur_s
         for (int i = 0; i < 8; ++i) bc[i] = (j == 7) ? c7[i] : cur_s[j * 8 + i];
         float w[K + 7];
         load_col(min(win.left + j, xmax), w);
+        float e[K];
 #pragma unroll
         for (int q = 0; q < K; ++q) {
             const float v = column_ssd_at<K>(bc, w, q);
+            e[q] = 0.0f;
             if (j >= 1) {
-                const float np = __fadd_rn(vp[q], v);          // P(j-1)
+                const float np = __fadd_rn(vp[q], v);  // P(j-1)
                 if (j >= 3) {
                     const float nq = __fadd_rn(pr[q][(j + 1) & 1], np);  // Q(j-3)
-                    if (j == 7) offer(__fadd_rn(qr[q][0], nq), q, 0);    // E(0)
+                    if (j == 7) e[q] = __fadd_rn(qr[q][0], nq);          // E(0)
                     qr[q][(j + 1) & 3] = nq;
                 }
                 pr[q][(j + 1) & 1] = np;
             }
             vp[q] = v;
         }
+        if (j == 7) emit(e, 0);
     }
-    // steady state: block column 7, steps j = 8 .. jcount-1 (4 per iteration,
-    // so the ring positions are static)
+    // steady state: block column 7, steps j = 8 .. jcount-1, four per
+    // iteration so that the ring positions are static
     for (int j0 = 8; j0 < jcount; j0 += 4) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int j = j0 + u;
             float w[K + 7];
             load_col(min(win.left + j, xmax), w);
+            float e[K];
 #pragma unroll
             for (int q = 0; q < K; ++q) {
                 const float v = column_ssd_at<K>(c7, w, q);
                 const float np = __fadd_rn(vp[q], v);
                 const float nq = __fadd_rn(pr[q][(u + 1) & 1], np);
-                const float e = __fadd_rn(qr[q][(u + 1) & 3], nq);
+                e[q] = __fadd_rn(qr[q][(u + 1) & 3], nq);
                 pr[q][(u + 1) & 1] = np;
                 qr[q][(u + 1) & 3] = nq;
                 vp[q] = v;
-                if (j < jcount) offer(e, q, j - 7);
             }
+            if (j < jcount) emit(e, j - 7);
         }
-        thr = umin64(thr, group_min(L.k[7], gmask));
+    }
+    // merge the rows' two smallest into the lane's 8 smallest
+#pragma unroll
+    for (int q = 0; q < 2 * K; ++q) {
+        float c = q < K ? m1[q] : m2[q - K];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            const float lo = fminf(lb[i], c);
+            c = fmaxf(lb[i], c);
+            lb[i] = lo;
+        }
     }
 }
 
-template <int K>
-__device__ __forceinline__ void scan_task(bool smem_ok, const Source& src, const float* cur_s,
-                                          const float c7[8], const Window& win, int r0, int nrows,
-                                          int jcount, int row_max, unsigned gmask, KeyList& L,
-                                          uint64_t& thr) {
-    if (smem_ok)
-        scan_chunk<K, true>(src, cur_s, c7, win, r0, nrows, jcount, row_max, gmask, L, thr);
-    else
-        scan_chunk<K, false>(src, cur_s, c7, win, r0, nrows, jcount, row_max, gmask, L, thr);
+__device__ __forceinline__ int rows_per_lane(int total_rows) {
+    return min(kMaxK, max(kMinK, (total_rows + 7) / 8));
 }
 
-// Scans windows[0..nwin) (rows split into chunks of K) into L. The windows
-// live in the group's shared memory; every lane of the group makes the same
-// choices (K, task count, source), so the group shuffles inside stay aligned.
-__device__ void scan_windows(int K, const Source& src, int rx1, int ry1, const float* cur_s,
-                             const float c7[8], const Window* wins, int nwin, int height,
-                             int sub, unsigned gmask, KeyList& L) {
+// A block's global match list, spatial predictors, the phase's top-8 and the
+// collection buffer (src/bm3d.comp:469-470, 541-545, 622-633).
+struct GroupState {
+    float ge[8];
+    uint32_t gxy[8];
+    int gz[8];
+    uint32_t sxy[8];
+    uint32_t pxy[8];
+    uint64_t top[8];
+    uint64_t buf[kCollect];
+    int count;
+};
+
+// The 8 smallest (error, scan index) keys of the windows' error table into
+// gs->top (padded with (FLT_MAX, INT_MAX) when fewer exist; errors >= FLT_MAX
+// never count, as in the reference). lb: this lane's 8 smallest per-row
+// minima (ascending). All 8 lanes of the group take part.
+__device__ void select_top8(const float* E, const Window* wins, int nwin, float lb[8],
+                            GroupState* gs, unsigned gmask) {
+    const int sub = threadIdx.x & 7;
+    // bound: the 8th smallest of the rows' two smallest errors -- at least 8
+    // candidates lie at or below it
+    float bound = kFltMax;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        float best = lb[0];
+        int src = sub;
+#pragma unroll
+        for (int off = 1; off < 8; off <<= 1) {
+            const float o = __shfl_xor_sync(gmask, best, off);
+            const int os = __shfl_xor_sync(gmask, src, off);
+            const bool take = o < best || (o == best && os < src);
+            best = take ? o : best;
+            src = take ? os : src;
+        }
+        bound = best;
+        if (sub == src) {
+#pragma unroll
+            for (int i = 0; i < 7; ++i) lb[i] = lb[i + 1];
+            lb[7] = kFltMax;
+        }
+    }
+    uint64_t tkey = (uint64_t(__float_as_uint(bound)) << 32) | 0xffffffffu;
+    int n;
+    for (;;) {
+        if (sub == 0) gs->count = 0;
+        __syncwarp(gmask);
+        const float terr = key_err(tkey);
+        const uint32_t tseq = uint32_t(tkey);
+        for (int wi = 0; wi < nwin; ++wi) {
+            const Window w = wins[wi];
+            for (int d = 0; d < w.rw; ++d) {
+                const float* col = E + w.eoff + d * w.h;
+                for (int row = sub; row < w.h; row += 8) {
+                    const float e = col[row];
+                    if (e <= terr && e < kFltMax) {
+                        const uint32_t seq = uint32_t(w.seq_base + row * w.rw + d);
+                        if (e < terr || seq <= tseq) {
+                            const int pos = atomicAdd(&gs->count, 1);
+                            if (pos < kCollect) gs->buf[pos] = make_key(e, int(seq));
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp(gmask);
+        n = gs->count;
+        if (n <= kCollect) break;
+        // more than kCollect at or below the bound: tighten it to the 8th
+        // smallest key among the collected ones and collect again
+        uint64_t t8 = kKeyMax;
+        for (int j = sub; j < kCollect; j += 8) {
+            const uint64_t kj = gs->buf[j];
+            int rank = 0;
+            for (int i = 0; i < kCollect; ++i) rank += gs->buf[i] < kj ? 1 : 0;
+            if (rank == 7) t8 = kj;
+        }
+#pragma unroll
+        for (int off = 1; off < 8; off <<= 1) {
+            const uint64_t o = __shfl_xor_sync(gmask, t8, off);
+            t8 = o < t8 ? o : t8;
+        }
+        tkey = t8;
+        __syncwarp(gmask);
+    }
+    gs->top[sub] = kKeyMax;
+    __syncwarp(gmask);
+    for (int j = sub; j < n; j += 8) {
+        const uint64_t kj = gs->buf[j];
+        int rank = 0;
+        for (int i = 0; i < n; ++i) rank += gs->buf[i] < kj ? 1 : 0;
+        if (rank < 8) gs->top[rank] = kj;
+    }
+    __syncwarp(gmask);
+}
+
+// Scans windows[0..nwin) of this lane's block into its error table, then
+// selects the top-8 into gs->top. Rows are split into chunks of K
+// (warp-uniform); chunk c of the block goes to lane c % 8 in round c / 8.
+__device__ void search_windows(const Region& reg, const float* cur_s, const float c7[8],
+                               const Window* wins, int nwin, float* E, GroupState* gs,
+                               unsigned gmask) {
+    const int sub = threadIdx.x & 7;
+    int total_rows = 0;
+    for (int i = 0; i < nwin; ++i) total_rows += wins[i].h;
+    const int K = warp_max(rows_per_lane(total_rows));
     int ntasks = 0;
     for (int i = 0; i < nwin; ++i) ntasks += (wins[i].h + K - 1) / K;
-    uint64_t thr = kKeyMax;
-    for (int t0 = 0; t0 < ntasks; t0 += 8) {
-        const int task = t0 + sub;
+    const int rounds = warp_max((ntasks + 7) / 8);
+    float lb[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) lb[i] = kFltMax;
+    for (int round = 0; round < rounds; ++round) {
+        const int task = round * 8 + sub;
         const bool has = task < ntasks;
         int wi = 0, c = has ? task : 0;
         while (wi < nwin - 1 && c >= (wins[wi].h + K - 1) / K) {
@@ -268,100 +322,113 @@ __device__ void scan_windows(int K, const Source& src, int rx1, int ry1, const f
         const Window win = wins[wi];
         const int r0 = win.top + c * K;
         const int nrows = has ? min(K, win.h - c * K) : 0;
-        const int jcount = group_max(has ? win.rw + 7 : 8, gmask);
-        const int row_max = min(win.top + win.h - 1 + 7, height - 1);
-        const bool inside = src.smem != nullptr && win.left >= src.rx0 &&
-                            win.left + win.rw + 6 <= rx1 && win.top >= src.ry0 && row_max <= ry1;
-        const bool smem_ok = __all_sync(gmask, inside);
-        thr = umin64(thr, group_min(L.k[7], gmask));
+        const int jcount = warp_max(has ? win.rw + 7 : 8);
         switch (K) {
-            case 2: scan_task<2>(smem_ok, src, cur_s, c7, win, r0, nrows, jcount, row_max, gmask, L, thr); break;
-            case 3: scan_task<3>(smem_ok, src, cur_s, c7, win, r0, nrows, jcount, row_max, gmask, L, thr); break;
-            case 4: scan_task<4>(smem_ok, src, cur_s, c7, win, r0, nrows, jcount, row_max, gmask, L, thr); break;
-            default: scan_task<5>(smem_ok, src, cur_s, c7, win, r0, nrows, jcount, row_max, gmask, L, thr); break;
+            case 2: scan_chunk<2>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
+            case 3: scan_chunk<3>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
+            case 4: scan_chunk<4>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
+            default: scan_chunk<5>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
         }
     }
-}
-
-__device__ __forceinline__ int rows_per_lane(int total_rows) {
-    return min(kMaxK, max(2, (total_rows + 7) / 8));
+    __syncwarp(gmask);
+    select_top8(E, wins, nwin, lb, gs, gmask);
 }
 
 // global list insertion of a temporal match (src/bm3d.comp:304-322)
 __device__ __forceinline__ void ginsert(float ge[8], uint32_t gxy[8], int gz[8], float err,
                                         uint32_t cxy, int cz) {
     if (err < ge[7]) {
-#pragma unroll
-        for (int k = 7; k > 0; --k) {
-            const bool sh = err < ge[k - 1];
-            const bool pl = err < ge[k];
-            ge[k] = sh ? ge[k - 1] : (pl ? err : ge[k]);
-            gxy[k] = sh ? gxy[k - 1] : (pl ? cxy : gxy[k]);
-            gz[k] = sh ? gz[k - 1] : (pl ? cz : gz[k]);
+        int pos = 7;
+        while (pos > 0 && err < ge[pos - 1]) {
+            ge[pos] = ge[pos - 1];
+            gxy[pos] = gxy[pos - 1];
+            gz[pos] = gz[pos - 1];
+            --pos;
         }
-        const bool p0 = err < ge[0];
-        ge[0] = p0 ? err : ge[0];
-        gxy[0] = p0 ? cxy : gxy[0];
-        gz[0] = p0 ? cz : gz[0];
+        ge[pos] = err;
+        gxy[pos] = cxy;
+        gz[pos] = cz;
     }
 }
 
-// Position of a merged key. Sentinels decode to (0, 0) as in the reference.
+// Position of a key. Sentinels decode to (0, 0) as in the reference.
 __device__ __forceinline__ uint32_t key_xy(uint64_t key, const Window* wins, int area) {
-    const uint32_t seq = uint32_t(key);
     if (key == kKeyMax) return 0u;
-    const int wi = area > 0 ? int(seq) / area : 0;
+    const int seq = int(uint32_t(key));
+    const int wi = area > 0 ? seq / area : 0;
     const Window w = wins[wi];
-    const int rem = int(seq) - w.seq_base;
+    const int rem = seq - w.seq_base;
     const int dy = rem / w.rw;
     const int dx = rem - dy * w.rw;
     return uint32_t(w.left + dx) | (uint32_t(w.top + dy) << 16);
 }
 
-// A block's global match list and predictors (src/bm3d.comp:469-470,541-545).
-struct GroupState {
-    float ge[8];
-    uint32_t gxy[8];
-    int gz[8];
-    uint32_t sxy[8];
-    uint32_t pxy[8];
-};
-
-// Stages frame rows [ry0, ry1] x columns [rx0, rx1] into smem (row stride ss).
+// Stages frame rows [ry0, ry1] x columns [rx0, rx1] into smem, column-major
+// with column stride cs (odd, so the transposing stores of a warp hit
+// distinct banks). Global reads are coalesced along rows.
 __device__ void stage_region(float* smem, const float* __restrict__ frame, int pitch, int rx0,
-                             int ry0, int rx1, int ry1, int ss) {
+                             int ry0, int rx1, int ry1, int cs) {
     const int w = rx1 - rx0 + 1;
     const int h = ry1 - ry0 + 1;
     const int lane = threadIdx.x & 31;
     for (int yy = threadIdx.x >> 5; yy < h; yy += blockDim.x >> 5) {
         const float* __restrict__ row = frame + (size_t)(ry0 + yy) * pitch + rx0;
-        for (int xx = lane; xx < w; xx += 32) smem[yy * ss + xx] = __ldg(row + xx);
+        for (int xx = lane; xx < w; xx += 32) smem[xx * cs + yy] = __ldg(row + xx);
     }
+}
+
+struct SmemPlan {
+    int region_floats;  // staged region
+    int estride;        // floats per block error table (== 8 mod 32)
+    size_t bytes;
+};
+
+__host__ __device__ inline int error_table_floats(const StackJob& job) {
+    const int ws = 2 * job.bm_range + 1, wt = 2 * job.ps_range + 1;
+    const int spatial = ws * ws;
+    const int temporal = job.radius > 0 ? job.ps_num * wt * wt : 0;
+    return spatial > temporal ? spatial : temporal;
+}
+
+__host__ __device__ inline SmemPlan smem_plan(const StackJob& job) {
+    SmemPlan p;
+    const int reach = job.bm_range + job.radius * job.ps_range;
+    const int tile_w = (kTileBX - 1) * job.step + 8, tile_h = (kTileBY - 1) * job.step + 8;
+    const int w = tile_w + 2 * reach < job.width ? tile_w + 2 * reach : job.width;
+    const int h = tile_h + 2 * reach < job.height ? tile_h + 2 * reach : job.height;
+    const int cs = (h + kMaxK + 7) | 1;
+    p.region_floats = cs * w;
+    p.estride = ((error_table_floats(job) + 31) & ~31) + 8;
+    p.bytes = sizeof(float) * (size_t(kGroups) * 64 + size_t(kGroups) * p.estride + p.region_floats) +
+              sizeof(Window) * kGroups * 8 + sizeof(GroupState) * kGroups;
+    return p;
 }
 
 }  // namespace
 
-// Shared memory: the block tiles' reference blocks (32 x 64 floats) followed
-// by the staged region.
-__global__ void __launch_bounds__(kMatchThreads, 1) bm3d_match_sliding_kernel(const StackJob job,
-                                                                          int region_floats) {
-    extern __shared__ float smem[];
-    constexpr int kGroups = kTileBX * kTileBY;
-    float* cur_all = smem;                                             // kGroups x 64
-    Window* win_all = reinterpret_cast<Window*>(smem + kGroups * 64);   // kGroups x 8
-    GroupState* gs_all = reinterpret_cast<GroupState*>(win_all + kGroups * 8);
-    float* region = reinterpret_cast<float*>(gs_all + kGroups);
+// Shared memory: block state, windows, reference blocks, error tables, then
+// the staged region.
+__global__ void __launch_bounds__(kMatchThreads, 1) bm3d_match_sliding_kernel(const StackJob job) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const SmemPlan plan = smem_plan(job);
+    GroupState* gs_all = reinterpret_cast<GroupState*>(smem_raw);
+    Window* win_all = reinterpret_cast<Window*>(gs_all + kGroups);
+    float* cur_all = reinterpret_cast<float*>(win_all + kGroups * 8);
+    float* etab_all = cur_all + kGroups * 64;
+    float* region = etab_all + (size_t)kGroups * plan.estride;
 
     const int lane = threadIdx.x & 31;
     const int sub = lane & 7;
-    const int g = threadIdx.x >> 3;
+    const int g = threadIdx.x >> 3;         // group in the CTA
+    const int wrp = g >> 2, gi = g & 3;     // warp, group in the warp
     const unsigned gmask = 0xffu << (lane & ~7);
     const int tiles_x = (job.nbx + kTileBX - 1) / kTileBX;
     const int tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
     const int bx0 = tx * kTileBX, by0 = ty * kTileBY;
     const int bx_last = min(bx0 + kTileBX - 1, job.nbx - 1);
     const int by_last = min(by0 + kTileBY - 1, job.nby - 1);
-    const int bxr = bx0 + (g % kTileBX), byr = by0 + (g / kTileBX);
+    // warp wrp: block row wrp/2, block columns (wrp&1) + {0, 2, 4, 6}
+    const int bxr = bx0 + (wrp & 1) + 2 * gi, byr = by0 + (wrp >> 1);
     const bool valid = bxr < job.nbx && byr < job.nby;
     const int bx = min(bxr, job.nbx - 1), by = min(byr, job.nby - 1);
     const int W = job.width, H = job.height;
@@ -373,96 +440,74 @@ __global__ void __launch_bounds__(kMatchThreads, 1) bm3d_match_sliding_kernel(co
     const int R = job.bm_range, Q = job.ps_range, P = job.ps_num;
     const int pitch = job.pitch;
 
-    // the reference block (column-major) and its column 7
     float* cur_s = cur_all + g * 64;
+    float* E = etab_all + (size_t)g * plan.estride;
     Window* win = win_all + g * 8;
+    GroupState* gs = gs_all + g;
     const float* fc = job.slice_frame[r];
-    {
-        const int c = sub;
 #pragma unroll
-        for (int i = 0; i < 8; ++i) cur_s[c * 8 + i] = __ldg(fc + (size_t)(y + i) * pitch + x + c);
-    }
-    __syncwarp();
+    for (int i = 0; i < 8; ++i) cur_s[sub * 8 + i] = __ldg(fc + (size_t)(y + i) * pitch + x + sub);
+    __syncwarp(gmask);
     float c7[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) c7[i] = cur_s[56 + i];
 
-    auto stage = [&](const float* frame, int reach, Source& s, int& rx1, int& ry1) {
+    auto stage = [&](const float* frame, int reach) {
+        Region s;
         const int rx0 = max(tile_x0 - reach, 0);
-        rx1 = min(tile_x1 + reach, W - 8) + 7;
+        const int rx1 = min(tile_x1 + reach, W - 8) + 7;
         const int ry0 = max(tile_y0 - reach, 0);
-        ry1 = min(tile_y1 + reach, H - 8) + 7;
-        const int ss = ((rx1 - rx0 + 1 + 31) & ~31) + 1;  // odd stride: rows hit distinct banks
-        s.frame = frame;
-        s.pitch = pitch;
+        const int ry1 = min(tile_y1 + reach, H - 8) + 7;
+        // column: the region's rows plus the rows masked chunk rows may read
+        s.cs = (ry1 - ry0 + 1 + kMaxK + 7) | 1;
         s.rx0 = rx0;
         s.ry0 = ry0;
-        s.ss = ss;
-        __syncthreads();  // previous phase finished reading the region
-        if ((ry1 - ry0 + 1 + kMaxK + 7) * ss <= region_floats) {
-            stage_region(region, frame, pitch, rx0, ry0, rx1, ry1, ss);
-            s.smem = region;
-        } else {
-            s.smem = nullptr;  // too large for shared memory: read the frame directly
-        }
+        s.smem = region;
+        __syncthreads();  // the previous phase has finished with the region
+        stage_region(region, frame, pitch, rx0, ry0, rx1, ry1, s.cs);
         __syncthreads();
+        return s;
     };
 
-    // the block's global match list, kept by lane 0 in shared memory
-    GroupState* gs = gs_all + g;
+    // spatial search (src/bm3d.comp:479-538)
     {
-        Source s;
-        int rx1, ry1;
-        stage(fc, R, s, rx1, ry1);
-        if (sub == 0) win[0] = make_window(x, y, R, W, H, 0);
+        const Region s = stage(fc, R);
+        if (sub == 0) win[0] = make_window(x, y, R, W, H, 0, 0);
         __syncwarp(gmask);
-        KeyList L;
-        L.reset();
-        scan_windows(rows_per_lane(win[0].h), s, rx1, ry1, cur_s, c7, win, 1, H, sub, gmask, L);
-        uint64_t mk[8];
-        merge_keys<8>(L, mk, 8, gmask);
-        if (sub == 0) {
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                gs->ge[k] = key_err(mk[k]);
-                gs->gxy[k] = key_xy(mk[k], win, 0);
-                gs->gz[k] = r;
-                gs->sxy[k] = gs->gxy[k];
-            }
-        }
+        search_windows(s, cur_s, c7, win, 1, E, gs, gmask);
+        const uint64_t k = gs->top[sub];
+        const uint32_t xy = key_xy(k, win, 0);
+        gs->ge[sub] = key_err(k);
+        gs->gxy[sub] = xy;
+        gs->gz[sub] = r;
+        gs->sxy[sub] = xy;
         __syncwarp(gmask);
     }
 
+    // temporal predictive search (src/bm3d.comp:540-637)
     const int area = (2 * Q + 1) * (2 * Q + 1);
     for (int dir = -1; dir <= 1; dir += 2) {
-        if (sub == 0)
-            for (int k = 0; k < 8; ++k) gs->pxy[k] = gs->sxy[k];
+        gs->pxy[sub] = gs->sxy[sub];
+        __syncwarp(gmask);
         for (int t = 1; t <= r; ++t) {
             const int z = r + dir * t;
-            Source s;
-            int rx1, ry1;
-            stage(job.slice_frame[z], R + t * Q, s, rx1, ry1);
-            if (sub == 0)
+            const Region s = stage(job.slice_frame[z], R + t * Q);
+            if (sub == 0) {
+                int eoff = 0;
                 for (int i = 0; i < P; ++i) {
                     const uint32_t p = gs->pxy[i];
-                    win[i] = make_window(int(p & 0xffffu), int(p >> 16), Q, W, H, i * area);
+                    win[i] = make_window(int(p & 0xffffu), int(p >> 16), Q, W, H, i * area, eoff);
+                    eoff += win[i].rw * win[i].h;
                 }
+            }
             __syncwarp(gmask);
-            int total_rows = 0;
-            for (int i = 0; i < P; ++i) total_rows += win[i].h;
-            KeyList L;
-            L.reset();
-            scan_windows(rows_per_lane(total_rows), s, rx1, ry1, cur_s, c7, win, P, H, sub, gmask, L);
-            uint64_t mk[8];
-            merge_keys<8>(L, mk, P, gmask);
+            search_windows(s, cur_s, c7, win, P, E, gs, gmask);
             if (sub == 0) {
-#pragma unroll
-                for (int i = 0; i < 8; ++i) {
-                    if (i < P) {
-                        const uint32_t fxy = key_xy(mk[i], win, area);
-                        ginsert(gs->ge, gs->gxy, gs->gz, key_err(mk[i]), fxy, z);
-                        gs->pxy[i] = fxy;
-                    }
+                for (int i = 0; i < P; ++i) {
+                    const uint64_t k = gs->top[i];
+                    const uint32_t fxy = key_xy(k, win, area);
+                    ginsert(gs->ge, gs->gxy, gs->gz, key_err(k), fxy, z);
+                    gs->pxy[i] = fxy;
                 }
             }
             __syncwarp(gmask);
@@ -499,32 +544,20 @@ __global__ void __launch_bounds__(kMatchThreads, 1) bm3d_match_sliding_kernel(co
 }
 
 namespace {
-constexpr int kRegionMaxFloats = 48 * 1024;  // 192 KB: larger regions read the frame directly
+constexpr size_t kSmemBudget = 220 * 1024;
 }
 
-// Shared memory for one tile: blocks, windows and the largest staged region
-// any phase needs (a full tile, reach bm_range + radius * ps_range).
-size_t match_sliding_smem(const StackJob& job, int* region_floats) {
-    const int reach = job.bm_range + job.radius * job.ps_range;
-    const int tile_w = (kTileBX - 1) * job.step + 8, tile_h = (kTileBY - 1) * job.step + 8;
-    const int w = std::min(tile_w + 2 * reach, job.width), h = std::min(tile_h + 2 * reach, job.height);
-    const int ss = ((w + 31) & ~31) + 1;
-    int floats = ss * (h + kMaxK + 7);  // + rows that masked chunk rows may read
-    if (floats > kRegionMaxFloats) floats = 0;
-    *region_floats = floats;
-    constexpr int kGroups = kTileBX * kTileBY;
-    return sizeof(float) * (kGroups * 64 + floats) + sizeof(Window) * kGroups * 8 +
-           sizeof(GroupState) * kGroups;
-}
+// True when the tiled kernel's shared memory holds this configuration;
+// otherwise the caller uses the direct-read kernel.
+bool match_sliding_fits(const StackJob& job) { return smem_plan(job).bytes <= kSmemBudget; }
 
 cudaError_t launch_match_sliding(const StackJob& job, cudaStream_t stream) {
-    int region_floats = 0;
-    const size_t smem = match_sliding_smem(job, &region_floats);
+    const size_t smem = smem_plan(job).bytes;
     cudaError_t e = cudaFuncSetAttribute(bm3d_match_sliding_kernel,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int tiles = ((job.nbx + kTileBX - 1) / kTileBX) * ((job.nby + kTileBY - 1) / kTileBY);
-    bm3d_match_sliding_kernel<<<tiles, kMatchThreads, smem, stream>>>(job, region_floats);
+    bm3d_match_sliding_kernel<<<tiles, kMatchThreads, smem, stream>>>(job);
     return cudaGetLastError();
 }
 
