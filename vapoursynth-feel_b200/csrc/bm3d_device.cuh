@@ -34,6 +34,7 @@ struct StackJob {
     float extractor;                   // 2^exp or 0
     uint32_t* match_xy;                // [nblocks][8]: x | y << 16
     uint32_t* match_z;                 // [nblocks]: 8 x 4-bit slice index
+    int* status;                       // device word, set nonzero on an internal error
 };
 
 // Per-output normalisation: numerator plane read at aggregation step i.

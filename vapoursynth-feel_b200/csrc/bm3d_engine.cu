@@ -254,6 +254,28 @@ struct vsfeel_bm3d {
     DevBuf<uint32_t> match_z;
     DevBuf<float> frames;     // staged input frames (host and frame paths)
     DevBuf<float> outbuf;     // staged output frames (host and frame paths)
+    DevBuf<int> status;       // kernels' internal-error word
+
+    int* status_word() {
+        if (!status.p) {
+            status.ensure(1);
+            VSF_CUDA(cudaMemset(status.p, 0, sizeof(int)));
+        }
+        return status.p;
+    }
+
+    // Waits for `st` (bounded) and reports an internal error the kernels flagged.
+    int finish(cudaStream_t st) {
+        const int rc = wait_stream(st, timeout_ms());
+        if (rc != VSFEEL_OK || !status.p) return rc;
+        int word = 0;
+        VSF_CUDA(cudaMemcpy(&word, status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (word != 0) {
+            VSF_CUDA(cudaMemset(status.p, 0, sizeof(int)));
+            return fail(VSFEEL_E_CUDA, "internal error: a search window left the staged region");
+        }
+        return VSFEEL_OK;
+    }
     std::map<int, int> frame_slot;  // frame cache of the per-frame path
     std::vector<int> slot_frame;
 
@@ -333,6 +355,7 @@ struct vsfeel_bm3d {
         job.extractor = s.extractor;
         job.match_xy = match_xy.p;
         job.match_z = match_z.p;
+        job.status = status_word();
         traced(VSFEEL_KERNEL_MATCH, st, [&] { return launch_match(job, st); });
         traced(VSFEEL_KERNEL_FILTER, st, [&] { return launch_filter(job, st); });
         launches += 2;
@@ -466,6 +489,7 @@ void vsfeel_bm3d_free(vsfeel_bm3d* ctx) {
         ctx->match_z.release();
         ctx->frames.release();
         ctx->outbuf.release();
+        ctx->status.release();
         for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     }
     delete ctx;
@@ -601,7 +625,7 @@ int vsfeel_bm3d_process_host(vsfeel_bm3d* ctx, const float* src, ptrdiff_t src_f
                                        dst_row_stride_bytes, ctx->outbuf.p + (size_t)q * ff,
                                        sizeof(float) * ctx->acc_pitch, row_bytes, s.height,
                                        cudaMemcpyDeviceToHost, st));
-        return wait_stream(st, timeout_ms());
+        return ctx->finish(st);
     });
 }
 
@@ -659,7 +683,7 @@ int vsfeel_bm3d_get_frame(vsfeel_bm3d* ctx, int n, vsfeel_fetch_fn fetch, vsfeel
                  ctx->acc_pitch, [&](int) { return ctx->outbuf.p; }, ctx->acc_pitch, n, 1, st);
         VSF_CUDA(cudaMemcpy2DAsync(dst, dst_stride_bytes, ctx->outbuf.p, sizeof(float) * ctx->acc_pitch,
                                    row_bytes, s.height, cudaMemcpyDeviceToHost, st));
-        return wait_stream(st, timeout_ms());
+        return ctx->finish(st);
     });
 }
 
@@ -681,7 +705,7 @@ int vsfeel_bm3d_match_table_device(vsfeel_bm3d* ctx, const float* src, int64_t s
         std::vector<uint32_t> xy((size_t)ctx->nblocks * 8), zz((size_t)ctx->nblocks);
         VSF_CUDA(cudaMemcpyAsync(xy.data(), ctx->match_xy.p, xy.size() * 4, cudaMemcpyDeviceToHost, st));
         VSF_CUDA(cudaMemcpyAsync(zz.data(), ctx->match_z.p, zz.size() * 4, cudaMemcpyDeviceToHost, st));
-        const int rc = wait_stream(st, timeout_ms());
+        const int rc = ctx->finish(st);
         if (rc != VSFEEL_OK) return rc;
         for (int b = 0; b < ctx->nblocks; ++b)
             for (int k = 0; k < 8; ++k) {

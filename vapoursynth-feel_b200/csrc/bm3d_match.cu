@@ -79,6 +79,7 @@ __device__ __forceinline__ Window make_window(int cx, int cy, int range, int wid
 struct Region {
     const float* smem;
     int rx0, ry0, cs;
+    int rx1, ry1;  // last staged column and row
 };
 
 // SSD of one column of the block (bc) against w[q..q+7].
@@ -248,17 +249,25 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
         __syncwarp(gmask);
         const float terr = key_err(tkey);
         const uint32_t tseq = uint32_t(tkey);
+        // a window's table is rw*h contiguous words from a 4-aligned offset:
+        // sweep it four entries per load, 32 per group step
         for (int wi = 0; wi < nwin; ++wi) {
             const Window w = wins[wi];
-            for (int d = 0; d < w.rw; ++d) {
-                const float* col = E + w.eoff + d * w.h;
-                for (int row = sub; row < w.h; row += 8) {
-                    const float e = col[row];
-                    if (e <= terr && e < kFltMax) {
+            const int n_w = w.rw * w.h;
+            const float4* tab = reinterpret_cast<const float4*>(E + w.eoff);
+            for (int v = sub; 4 * v < n_w; v += 8) {
+                const float4 q = tab[v];
+                const float ev[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int f = 4 * v + u;
+                    if (f < n_w && ev[u] <= terr && ev[u] < kFltMax) {
+                        const int d = f / w.h;
+                        const int row = f - d * w.h;
                         const uint32_t seq = uint32_t(w.seq_base + row * w.rw + d);
-                        if (e < terr || seq <= tseq) {
+                        if (ev[u] < terr || seq <= tseq) {
                             const int pos = atomicAdd(&gs->count, 1);
-                            if (pos < kCollect) gs->buf[pos] = make_key(e, int(seq));
+                            if (pos < kCollect) gs->buf[pos] = make_key(ev[u], int(seq));
                         }
                     }
                 }
@@ -300,7 +309,7 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
 // (warp-uniform); chunk c of the block goes to lane c % 8 in round c / 8.
 __device__ void search_windows(const Region& reg, const float* cur_s, const float c7[8],
                                const Window* wins, int nwin, float* E, GroupState* gs,
-                               unsigned gmask) {
+                               unsigned gmask, int* status) {
     const int sub = threadIdx.x & 7;
     int total_rows = 0;
     for (int i = 0; i < nwin; ++i) total_rows += wins[i].h;
@@ -319,9 +328,19 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
             c -= (wins[wi].h + K - 1) / K;
             ++wi;
         }
-        const Window win = wins[wi];
-        const int r0 = win.top + c * K;
-        const int nrows = has ? min(K, win.h - c * K) : 0;
+        Window win = wins[wi];
+        int r0 = win.top + c * K;
+        int nrows = has ? min(K, win.h - c * K) : 0;
+        // every window lies inside the staged region by construction (the
+        // host routes configurations that could place one outside to the
+        // direct-read kernel); should one not, scan nothing here and report
+        if (win.left < reg.rx0 || win.left + win.rw + 6 > reg.rx1 || win.top < reg.ry0 ||
+            win.top + win.h + 6 > reg.ry1) {
+            if (has) atomicOr(status, 1);
+            win = Window{reg.rx0, reg.ry0, 1, 1, 0, 0};
+            r0 = reg.ry0;
+            nrows = 0;
+        }
         const int jcount = warp_max(has ? win.rw + 7 : 8);
         switch (K) {
             case 2: scan_chunk<2>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
@@ -385,8 +404,8 @@ struct SmemPlan {
 
 __host__ __device__ inline int error_table_floats(const StackJob& job) {
     const int ws = 2 * job.bm_range + 1, wt = 2 * job.ps_range + 1;
-    const int spatial = ws * ws;
-    const int temporal = job.radius > 0 ? job.ps_num * wt * wt : 0;
+    const int spatial = (ws * ws + 3) & ~3;
+    const int temporal = job.radius > 0 ? job.ps_num * ((wt * wt + 3) & ~3) : 0;
     return spatial > temporal ? spatial : temporal;
 }
 
@@ -462,6 +481,8 @@ __global__ void __launch_bounds__(kMatchThreads, 1) bm3d_match_sliding_kernel(co
         s.cs = (ry1 - ry0 + 1 + kMaxK + 7) | 1;
         s.rx0 = rx0;
         s.ry0 = ry0;
+        s.rx1 = rx1;
+        s.ry1 = ry1;
         s.smem = region;
         __syncthreads();  // the previous phase has finished with the region
         stage_region(region, frame, pitch, rx0, ry0, rx1, ry1, s.cs);
@@ -474,7 +495,7 @@ __global__ void __launch_bounds__(kMatchThreads, 1) bm3d_match_sliding_kernel(co
         const Region s = stage(fc, R);
         if (sub == 0) win[0] = make_window(x, y, R, W, H, 0, 0);
         __syncwarp(gmask);
-        search_windows(s, cur_s, c7, win, 1, E, gs, gmask);
+        search_windows(s, cur_s, c7, win, 1, E, gs, gmask, job.status);
         const uint64_t k = gs->top[sub];
         const uint32_t xy = key_xy(k, win, 0);
         gs->ge[sub] = key_err(k);
@@ -497,11 +518,11 @@ __global__ void __launch_bounds__(kMatchThreads, 1) bm3d_match_sliding_kernel(co
                 for (int i = 0; i < P; ++i) {
                     const uint32_t p = gs->pxy[i];
                     win[i] = make_window(int(p & 0xffffu), int(p >> 16), Q, W, H, i * area, eoff);
-                    eoff += win[i].rw * win[i].h;
+                    eoff += (win[i].rw * win[i].h + 3) & ~3;  // tables start 4-aligned
                 }
             }
             __syncwarp(gmask);
-            search_windows(s, cur_s, c7, win, P, E, gs, gmask);
+            search_windows(s, cur_s, c7, win, P, E, gs, gmask, job.status);
             if (sub == 0) {
                 for (int i = 0; i < P; ++i) {
                     const uint64_t k = gs->top[i];
@@ -547,9 +568,21 @@ namespace {
 constexpr size_t kSmemBudget = 220 * 1024;
 }
 
-// True when the tiled kernel's shared memory holds this configuration;
-// otherwise the caller uses the direct-read kernel.
-bool match_sliding_fits(const StackJob& job) { return smem_plan(job).bytes <= kSmemBudget; }
+// True when the tiled kernel handles this configuration: its shared memory
+// fits, and every temporal window is centred on a real match. (A corner
+// block's spatial window holds (min(R, W-8)+1) * (min(R, H-8)+1) candidates;
+// with fewer than ps_num of them the reference seeds a temporal window at
+// (0, 0), which can lie outside the tile's staged region.) Otherwise the
+// caller uses the direct-read kernel.
+bool match_sliding_fits(const StackJob& job) {
+    if (smem_plan(job).bytes > kSmemBudget) return false;
+    if (job.radius > 0) {
+        const int cw = std::min(job.bm_range, job.width - 8) + 1;
+        const int ch = std::min(job.bm_range, job.height - 8) + 1;
+        if (cw * ch < job.ps_num) return false;
+    }
+    return true;
+}
 
 cudaError_t launch_match_sliding(const StackJob& job, cudaStream_t stream) {
     const size_t smem = smem_plan(job).bytes;
