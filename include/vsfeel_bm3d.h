@@ -157,6 +157,31 @@ VSFEEL_API int vsfeel_bm3d_trace(vsfeel_bm3d* ctx, int enable);
 VSFEEL_API int vsfeel_bm3d_trace_read(vsfeel_bm3d* ctx, double ms[VSFEEL_KERNEL_KINDS],
                                       int64_t launches[VSFEEL_KERNEL_KINDS]);
 
+/* Allocation-free form of vsfeel_bm3d_process_device; it has no counterpart
+ * in the reference. It is for callers that cannot let this library allocate
+ * device memory: processes that reserve the GPU's memory in their own fixed
+ * pools up front, and real-time pipelines that must not pay the implicit
+ * device synchronisation of cudaMalloc/cudaFree. It takes the arguments and
+ * clip format directly (no context), reads src and writes dst as
+ * process_device does, and keeps every intermediate in one static device
+ * array of vsfeel_bm3d_noalloc_scratch_bytes() (32 MiB), held by every GPU
+ * that loads the library until exit; clips whose match table and
+ * accumulator planes need more are rejected with an error. The first call
+ * on each device resolves the array's device address, so make it before any
+ * stream capture. The call only enqueues work on `stream` (used as given)
+ * and never waits. All calls share the array: calls that overlap on the GPU
+ * race and must be serialised by the caller. */
+VSFEEL_API int vsfeel_bm3d_process_device_noalloc(const vsfeel_bm3d_args* args,
+                                                  const vsfeel_bm3d_video_info* vi,
+                                                  const float* src, int64_t src_frame_stride,
+                                                  int64_t src_row_stride, float* dst,
+                                                  int64_t dst_frame_stride,
+                                                  int64_t dst_row_stride, int first, int count,
+                                                  void* stream);
+
+/* Size of the allocation-free entry point's static scratch array, bytes. */
+VSFEEL_API int64_t vsfeel_bm3d_noalloc_scratch_bytes(void);
+
 /* The calling thread's last error message ("" when none). */
 VSFEEL_API const char* vsfeel_bm3d_last_error(void);
 

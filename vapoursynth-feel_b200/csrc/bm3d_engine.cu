@@ -433,6 +433,38 @@ int guarded(vsfeel_bm3d* ctx, F&& fn) {
 
 }  // namespace
 
+namespace vsfeel {
+
+// Validates arguments as vsfeel_bm3d_create does and reports the effective
+// parameters, without touching the device (used by the allocation-free entry
+// point in bm3d_noalloc.cu).
+int parse_to_info(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
+                  vsfeel_bm3d_info* info) {
+    Settings s;
+    const int rc = parse_args(args, vi, s);
+    if (rc != VSFEEL_OK) return rc;
+    std::memset(info, 0, sizeof(*info));
+    info->width = s.width;
+    info->height = s.height;
+    info->num_frames = s.nframes;
+    info->radius = s.radius;
+    info->block_step = s.step;
+    info->bm_range = s.bm_range;
+    info->ps_num = s.ps_num;
+    info->ps_range = s.ps_range;
+    info->num_streams = s.num_streams;
+    info->sigma = s.sigma;
+    info->threshold = s.thr;
+    info->extractor = s.extractor;
+    info->blocks_x = block_count(s.width, s.step);
+    info->blocks_y = block_count(s.height, s.step);
+    return VSFEEL_OK;
+}
+
+int set_error(int code, const char* msg) { return fail(code, msg); }
+
+}  // namespace vsfeel
+
 extern "C" {
 
 int vsfeel_bm3d_abi_version(void) { return VSFEEL_BM3D_ABI_VERSION; }

@@ -17,7 +17,7 @@ CSRC = Path(__file__).resolve().parent
 PKG = CSRC.parent / "vsfeel"
 INCLUDE = CSRC.parent.parent / "include"
 LIB = PKG / "libvsfeel_bm3d.so"
-SOURCES = ["bm3d_kernels.cu", "bm3d_match.cu", "bm3d_engine.cu"]
+SOURCES = ["bm3d_kernels.cu", "bm3d_match.cu", "bm3d_engine.cu", "bm3d_noalloc.cu"]
 HEADERS = ["bm3d_device.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")

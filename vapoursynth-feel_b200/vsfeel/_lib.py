@@ -28,6 +28,8 @@ EXPORTS = (
     "vsfeel_bm3d_launch_count",
     "vsfeel_bm3d_trace",
     "vsfeel_bm3d_trace_read",
+    "vsfeel_bm3d_process_device_noalloc",
+    "vsfeel_bm3d_noalloc_scratch_bytes",
     "vsfeel_bm3d_last_error",
     "vsfeel_bm3d_abi_version",
 )
@@ -140,6 +142,12 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.vsfeel_bm3d_trace_read.argtypes = [c_p, ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(c_i64)]
     lib.vsfeel_bm3d_trace_read.restype = c_int
+    lib.vsfeel_bm3d_process_device_noalloc.argtypes = [ctypes.POINTER(Args),
+                                                       ctypes.POINTER(VideoInfo), c_p, c_i64,
+                                                       c_i64, c_p, c_i64, c_i64, c_int, c_int, c_p]
+    lib.vsfeel_bm3d_process_device_noalloc.restype = c_int
+    lib.vsfeel_bm3d_noalloc_scratch_bytes.argtypes = []
+    lib.vsfeel_bm3d_noalloc_scratch_bytes.restype = c_i64
     lib.vsfeel_bm3d_last_error.argtypes = []
     lib.vsfeel_bm3d_last_error.restype = ctypes.c_char_p
     lib.vsfeel_bm3d_abi_version.argtypes = []
