@@ -155,6 +155,73 @@ def cpu_baseline_port(luma):
                       f"1920x1080 r2 workload, oracle fp32 with {threads} threads, {dt:.1f} s"}
 
 
+GRAD_WORKLOADS = {
+    # the differentiable workload: 16 frames 512x512, radius 1
+    "fwd_bwd_512x512x16_r1": dict(frames=16, height=512, width=512, shift=3, seed=4,
+                                  params=dict(sigma=5.0, block_step=4, bm_range=12, radius=1,
+                                              ps_num=2, ps_range=5)),
+    # the plain workload's clip and settings, forward + backward
+    "fwd_bwd_1920x1080x32_r2": dict(frames=32, height=HEIGHT, width=WIDTH, shift=4, seed=2000,
+                                    params=dict(PARAMS)),
+}
+
+
+def time_fwd_bwd(torch, dev, name, steps, warmup):
+    """Forward alone (the plain path) and forward+backward through the
+    autograd Function on one workload, timed with CUDA events; loss =
+    sum(W * out) with W ~ N(0, 1) seeded."""
+    import vsfeel
+    from vsfeel.autograd import Denoiser
+    from vsfeel.synthetic import make_clip
+
+    wl = GRAD_WORKLOADS[name]
+    n, h, w = wl["frames"], wl["height"], wl["width"]
+    frames = make_clip(n, h, w, sigma=wl["params"]["sigma"], shift=wl["shift"], seed=wl["seed"])
+    x = torch.from_numpy(frames).to(dev)
+    weights = torch.randn(x.shape, generator=torch.Generator(device=dev).manual_seed(6),
+                          device=dev)
+    node = vsfeel.BM3Dv2(vsfeel.clip_from_array(frames), device=dev.index, **wl["params"])
+    den = Denoiser(x.shape, dev.index, **wl["params"])
+    plain = torch.empty_like(x)
+
+    def fwd():
+        node.output_device(x, plain)
+
+    def fwd_bwd():
+        xr = x.detach().requires_grad_(True)
+        out = den(xr)
+        out.backward(weights)
+        return xr.grad
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(steps):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / steps
+
+    torch.cuda.reset_peak_memory_stats(dev)
+    free0, total = torch.cuda.mem_get_info(dev)
+    fwd_ms = timed(fwd)
+    fb_ms = timed(fwd_bwd)
+    # adjoint kernel alone
+    out, saved = den.forward_saved(x)
+    torch.cuda.synchronize()
+    adj_ms = timed(lambda: den.backward(saved, weights))
+    px = n * h * w
+    return {"workload": name, "fwd_mpx_s": px / fwd_ms / 1e3, "fwd_bwd_mpx_s": px / fb_ms / 1e3,
+            "fwd_ms": fwd_ms, "fwd_bwd_ms": fb_ms, "backward_only_ms": adj_ms,
+            "fwd_bwd_over_fwd": fb_ms / fwd_ms, "saved_state_bytes": int(den.layout.bytes),
+            "torch_peak_bytes": int(torch.cuda.max_memory_allocated(dev)),
+            "library_bytes": int(den.info.device_bytes + node.info.device_bytes),
+            "steps": steps, "warmup": warmup}
+
+
 def run_reference(args) -> int:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -220,6 +287,8 @@ def main() -> int:
                     help="frames per step (default 32; smaller only for profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass")
+    ap.add_argument("--no-grad", action="store_true",
+                    help="skip the forward+backward measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -338,6 +407,9 @@ def main() -> int:
         "roofline": roofline,
         "clocks": clk,
     }
+    if world == 1 and not args.no_grad:
+        line["fwd_bwd"] = [time_fwd_bwd(torch, dev, name, max(3, args.steps // 2), 3)
+                           for name in GRAD_WORKLOADS]
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(luma)
     print(json.dumps(line), flush=True)

@@ -149,13 +149,57 @@ VSFEEL_API int64_t vsfeel_bm3d_launch_count(const vsfeel_bm3d* ctx);
  * reference's BM3D_GPUTRACE, src/bm3d.cpp:978-994). enable != 0 starts (and
  * resets) the trace, 0 stops it. */
 enum { VSFEEL_KERNEL_MATCH = 0, VSFEEL_KERNEL_FILTER = 1, VSFEEL_KERNEL_NORMALIZE = 2,
-       VSFEEL_KERNEL_KINDS = 3 };
+       VSFEEL_KERNEL_ADJOINT = 3, VSFEEL_KERNEL_KINDS = 4 };
 VSFEEL_API int vsfeel_bm3d_trace(vsfeel_bm3d* ctx, int enable);
 
 /* Waits for the traced work, then returns per kernel kind the summed device
  * milliseconds and the number of traced launches. */
 VSFEEL_API int vsfeel_bm3d_trace_read(vsfeel_bm3d* ctx, double ms[VSFEEL_KERNEL_KINDS],
                                       int64_t launches[VSFEEL_KERNEL_KINDS]);
+
+/* ---- Differentiable form (no counterpart in the reference) --------------
+ *
+ * The forward pass of a whole clip that also records what its adjoint needs,
+ * and the adjoint: dLoss/dInput from dLoss/dOutput with the match table, the
+ * threshold keep masks and the aggregation weights frozen at the forward
+ * pass. With those frozen the denoiser is linear in its input, and the
+ * adjoint applies the transpose of that linear map (the 3D spectra are
+ * recomputed from the saved match table, not stored). The extractor's
+ * rounding of the scattered values (extractor_exp != 0) is taken as the
+ * identity. Both calls cover the whole clip (outputs 0 .. num_frames-1) with
+ * device buffers (strides in floats) and only enqueue work on `stream`.
+ *
+ * The saved state is one caller-owned device buffer of `bytes`, 256-byte
+ * aligned: for each stack m a record at m * stack_bytes holding
+ *   match_xy_offset: [num_blocks][8] uint32, x | y << 16 of each match
+ *   match_z_offset:  [num_blocks] uint32, 4 bits per match: its slice z
+ *   mask_offset:     [num_blocks][8] uint64; word h, bit 8*g + v is set
+ *                    when the 3D coefficient of group frequency g, vertical
+ *                    frequency v and horizontal frequency h was kept
+ * then, at den_offset, the frozen denominators: float planes of output n at
+ * n * den_frame_stride floats, rows den_row_stride floats apart. Blocks are
+ * in raster order of the block grid. */
+typedef struct vsfeel_bm3d_saved_info {
+    int64_t bytes, stack_bytes;
+    int64_t match_xy_offset, match_z_offset, mask_offset;
+    int64_t den_offset, den_row_stride, den_frame_stride;
+    int64_t num_blocks;
+} vsfeel_bm3d_saved_info;
+
+VSFEEL_API int vsfeel_bm3d_saved_layout(const vsfeel_bm3d* ctx, vsfeel_bm3d_saved_info* out);
+
+/* Denoises every frame of the clip like process_device and writes the saved
+ * state into `saved` (vsfeel_bm3d_saved_layout().bytes). */
+VSFEEL_API int vsfeel_bm3d_forward_saved(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
+                                         int64_t src_row_stride, float* dst,
+                                         int64_t dst_frame_stride, int64_t dst_row_stride,
+                                         void* saved, void* stream);
+
+/* Writes dLoss/dInput into grad_in (overwritten) from dLoss/dOutput and the
+ * saved state of a forward_saved call of the same context. */
+VSFEEL_API int vsfeel_bm3d_backward(vsfeel_bm3d* ctx, const void* saved, const float* grad_out,
+                                    int64_t go_frame_stride, int64_t go_row_stride, float* grad_in,
+                                    int64_t gi_frame_stride, int64_t gi_row_stride, void* stream);
 
 /* Allocation-free form of vsfeel_bm3d_process_device; it has no counterpart
  * in the reference. It is for callers that cannot let this library allocate

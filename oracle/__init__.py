@@ -80,6 +80,9 @@ class Oracle:
         lib.oracle_bm3d_f64.restype = _i
         lib.oracle_bm3d_matches_f32.argtypes = [_p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i, _i, _p]
         lib.oracle_bm3d_matches_f32.restype = _i
+        lib.oracle_bm3d_frozen_state.argtypes = [_p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i,
+                                                 _i, _i, _p, _p]
+        lib.oracle_bm3d_frozen_state.restype = _i
         lib.oracle_bm3d_stack_f32.argtypes = [_p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i, _i, _i, _p]
         lib.oracle_bm3d_stack_f32.restype = _i
         lib.oracle_block_count.argtypes = [_i, _i, _i]
@@ -119,6 +122,21 @@ class Oracle:
         if rc != 0:
             raise ValueError("oracle rejected the arguments")
         return table
+
+    def frozen_state(self, frames, params: Params, m: int, fp64=False, nthreads=None):
+        """(match table [nblocks, 8, 3] int32, keep bits [nblocks, 8] uint64) of
+        stack m, in the layout of the library's saved state."""
+        a = _frames(frames)
+        n, h, w = a.shape
+        nb = self.block_count(w, h, params.block_step)
+        table = np.empty((nb, 8, 3), dtype=np.int32)
+        keep = np.empty((nb, 8), dtype=np.uint64)
+        rc = self.lib.oracle_bm3d_frozen_state(_ptr(a), n, w, h, *params.args(), m,
+                                               1 if fp64 else 0, nthreads or _default_threads(),
+                                               _ptr(table), _ptr(keep))
+        if rc != 0:
+            raise ValueError("oracle rejected the arguments")
+        return table, keep
 
     def stack(self, frames, params: Params, m: int, nthreads=None) -> np.ndarray:
         a = _frames(frames)

@@ -372,8 +372,10 @@ void match_block(const Params& P, const Frames& F, int m, int x, int y, int out[
 // X[k][a][b]: group member k, row a, column b. The 1-D transforms run in the
 // reference's order: rows-of-columns, columns-of-rows, then along the group;
 // the inverse runs in the same axis order.
+// keep (optional): receives the keep bits, word b (horizontal frequency),
+// bit 8*k + a (group frequency k, vertical frequency a).
 template <class T>
-T filter_group(const Params& P, T X[8][8][8]) {
+T filter_group(const Params& P, T X[8][8][8], uint64_t* keep_bits = nullptr) {
     T v[8];
     for (int k = 0; k < 8; ++k)
         for (int b = 0; b < 8; ++b) {
@@ -392,6 +394,8 @@ T filter_group(const Params& P, T X[8][8][8]) {
 
     const T thr = T(P.thr);
     int kept = 0;
+    if (keep_bits)
+        for (int b = 0; b < 8; ++b) keep_bits[b] = 0;
     for (int k = 0; k < 8; ++k)
         for (int a = 0; a < 8; ++a)
             for (int b = 0; b < 8; ++b) {
@@ -399,6 +403,7 @@ T filter_group(const Params& P, T X[8][8][8]) {
                 const T t = (k == 0 && a == 0 && b == 0) ? T(0) : thr;
                 const bool keep = std::fabs(val) >= t;
                 kept += keep ? 1 : 0;
+                if (keep_bits && keep) keep_bits[b] |= uint64_t(1) << (8 * k + a);
                 X[k][a][b] = keep ? val * (T(1) / T(4096)) : T(0);
             }
     const T weight = T(1) / T(kept);
@@ -425,6 +430,7 @@ struct BlockResult {
     int match[8][3];
     T X[8][8][8];
     T weight;
+    uint64_t keep[8];
 };
 
 int count_blocks(int extent, int step) { return (extent - 9 + 2 * step) / step; }
@@ -435,7 +441,7 @@ int count_blocks(int extent, int step) { return (extent - 9 + 2 * step) / step; 
 // columns, then lane (block column), member, row.
 template <class T>
 void run_stack(const Params& P, const Frames& F, int m, T* slices, int nthreads,
-               int32_t* match_out) {
+               int32_t* match_out, uint64_t* keep_out = nullptr) {
     const int nbx = count_blocks(P.width, P.step);
     const int nby = count_blocks(P.height, P.step);
     const size_t plane = (size_t)P.height * P.stride;
@@ -463,7 +469,7 @@ void run_stack(const Params& P, const Frames& F, int m, T* slices, int nthreads,
                                 br.X[k][a][b] =
                                     T(f[(size_t)(br.match[k][1] + a) * P.stride + br.match[k][0] + b]);
                     }
-                    br.weight = filter_group<T>(P, br.X);
+                    br.weight = filter_group<T>(P, br.X, br.keep);
                 }
             }
         };
@@ -483,6 +489,9 @@ void run_stack(const Params& P, const Frames& F, int m, T* slices, int nthreads,
                     for (int k = 0; k < 8; ++k)
                         for (int q = 0; q < 3; ++q) mo[k * 3 + q] = br.match[k][q];
                 }
+                if (keep_out)
+                    for (int b = 0; b < 8; ++b)
+                        keep_out[((size_t)(by0 + ry) * nbx + bx) * 8 + b] = br.keep[b];
                 if (!slices) continue;
                 const T wv = (br.weight + E) - E;
                 for (int b = 0; b < 8; ++b)
@@ -615,6 +624,26 @@ int oracle_bm3d_matches_f32(const float* frames, int nframes, int width, int hei
     if (m < 0 || m >= nframes) return -1;
     Frames F{frames, (size_t)height * width, nframes};
     run_stack<float>(P, F, m, nullptr, nthreads, table);
+    return 0;
+}
+
+// Frozen state of stack m for the differentiable form's tests: the match
+// table (as oracle_bm3d_matches_f32) and the keep bits of every group,
+// nblocks x 8 words (word = horizontal frequency, bit 8 * group frequency +
+// vertical frequency), in FP32 or FP64 arithmetic.
+int oracle_bm3d_frozen_state(const float* frames, int nframes, int width, int height, float sigma,
+                             int block_step, int bm_range, int radius, int ps_num, int ps_range,
+                             int m, int fp64, int nthreads, int32_t* table, uint64_t* keep) {
+    Params P;
+    if (!make_params(P, nframes, width, height, sigma, block_step, bm_range, radius, ps_num,
+                     ps_range, 0))
+        return -1;
+    if (m < 0 || m >= nframes) return -1;
+    Frames F{frames, (size_t)height * width, nframes};
+    if (fp64)
+        run_stack<double>(P, F, m, nullptr, nthreads, table, keep);
+    else
+        run_stack<float>(P, F, m, nullptr, nthreads, table, keep);
     return 0;
 }
 

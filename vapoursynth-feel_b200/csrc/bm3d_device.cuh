@@ -34,6 +34,7 @@ struct StackJob {
     float extractor;                   // 2^exp or 0
     uint32_t* match_xy;                // [nblocks][8]: x | y << 16
     uint32_t* match_z;                 // [nblocks]: 8 x 4-bit slice index
+    uint64_t* mask_out;                // [nblocks][8] keep bits of the filter, or null
     int* status;                       // device word, set nonzero on an internal error
 };
 
@@ -43,6 +44,28 @@ struct NormalizeJob {
     int64_t den_offset;  // floats from a numerator plane to its weight plane
     int tw, width, height, src_pitch, out_pitch;
     float* out;
+    float* den_out;  // summed weights (the frozen denominator), or null
+    int den_pitch;
+};
+
+// Adjoint of the frozen-match operator over a whole clip: one launch covers
+// every block of every stack. The saved state is what the forward pass
+// recorded per stack (match table and keep bits) plus the per-output
+// denominators.
+struct AdjointJob {
+    const unsigned char* saved;  // stack m's record at saved + m * stack_bytes
+    int64_t stack_bytes, off_xy, off_z, off_mask;
+    const float* den;            // [N] planes of den_pitch floats per row
+    int64_t den_frame;
+    int den_pitch;
+    const float* grad_out;       // dL/d(output), frame f at grad_out + f * go_frame
+    int64_t go_frame;
+    int go_pitch;
+    float* grad_in;              // dL/d(input), accumulated (zero-filled by the caller)
+    int64_t gi_frame;
+    int gi_pitch;
+    int nframes, radius, nblocks;
+    int width, height;           // match positions are clamped to the frame
 };
 
 // Host-side launchers (defined beside the kernels). Each returns the launch
@@ -52,9 +75,35 @@ cudaError_t launch_match_sliding(const StackJob& job, cudaStream_t stream);
 bool match_sliding_fits(const StackJob& job);
 cudaError_t launch_filter(const StackJob& job, cudaStream_t stream);
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream);
+cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream);
 
 __host__ __device__ inline int block_count(int extent, int step) {
     return (extent - 9 + 2 * step) / step;  // positions x0 = b*step < extent - 8 + step
+}
+
+__host__ __device__ inline int clamp_frame(int f, int nframes) {
+    return f < 0 ? 0 : (f > nframes - 1 ? nframes - 1 : f);
+}
+
+// Aggregation slice that output n reads from stack clamp(n - r + i)
+// (src/bm3d.cpp:369-371).
+__host__ __device__ inline int agg_slice(int i, int n, int nframes, int radius) {
+    if (radius == 0) return 0;
+    const int a = 2 * radius - i, b = n - nframes + 1 + radius;
+    const int lo = a > b ? a : b;
+    return lo < n + radius ? lo : n + radius;
+}
+
+// How many times output n = clamp(m - r + z) sums slice z of stack m: the
+// number of steps i with (clamp(n - r + i), agg_slice(i, n)) == (m, z). It
+// is 0 for slices no output reads and above 1 only near the clip ends.
+__host__ __device__ inline int slice_reads(int m, int z, int nframes, int radius) {
+    const int n = clamp_frame(m - radius + z, nframes);
+    int count = 0;
+    for (int i = 0; i <= 2 * radius; ++i)
+        if (clamp_frame(n - radius + i, nframes) == m && agg_slice(i, n, nframes, radius) == z)
+            ++count;
+    return count;
 }
 
 // ---------------------------------------------------------------------------

@@ -328,8 +328,28 @@ struct vsfeel_bm3d {
         return -1;
     }
 
+    // Saved state of the differentiable form: per stack a record of the
+    // match table and the keep bits, then the per-output denominators.
+    struct SavedLayout {
+        int64_t off_xy, off_z, off_mask, stack_bytes, den_offset, den_pitch, bytes;
+    };
+    SavedLayout saved_layout() const {
+        auto al = [](int64_t v) { return (v + 255) & ~int64_t(255); };
+        SavedLayout L{};
+        L.off_xy = 0;
+        L.off_z = al(L.off_xy + 4 * 8 * (int64_t)nblocks);
+        L.off_mask = al(L.off_z + 4 * (int64_t)nblocks);
+        L.stack_bytes = al(L.off_mask + 8 * 8 * (int64_t)nblocks);
+        L.den_offset = L.stack_bytes * s.nframes;
+        L.den_pitch = acc_pitch;
+        L.bytes = L.den_offset + 4 * (int64_t)s.nframes * s.height * acc_pitch;
+        return L;
+    }
+
+    // `saved` (the differentiable form): write stack m's match table and keep
+    // bits into its record instead of the context's match buffers.
     void launch_stack(int m, const std::function<const float*(int)>& frame_ptr, int in_pitch,
-                      int out_lo, int out_hi, cudaStream_t st) {
+                      int out_lo, int out_hi, cudaStream_t st, unsigned char* saved = nullptr) {
         const int r = s.radius;
         StackJob job{};
         for (int z = 0; z < tw(); ++z) {
@@ -355,13 +375,22 @@ struct vsfeel_bm3d {
         job.extractor = s.extractor;
         job.match_xy = match_xy.p;
         job.match_z = match_z.p;
+        job.mask_out = nullptr;
+        if (saved) {
+            const SavedLayout L = saved_layout();
+            unsigned char* rec = saved + (size_t)m * L.stack_bytes;
+            job.match_xy = reinterpret_cast<uint32_t*>(rec + L.off_xy);
+            job.match_z = reinterpret_cast<uint32_t*>(rec + L.off_z);
+            job.mask_out = reinterpret_cast<uint64_t*>(rec + L.off_mask);
+        }
         job.status = status_word();
         traced(VSFEEL_KERNEL_MATCH, st, [&] { return launch_match(job, st); });
         traced(VSFEEL_KERNEL_FILTER, st, [&] { return launch_filter(job, st); });
         launches += 2;
     }
 
-    void launch_normalize(int n, float* out, int out_pitch, cudaStream_t st) {
+    void launch_normalize(int n, float* out, int out_pitch, cudaStream_t st,
+                          unsigned char* saved = nullptr) {
         const int r = s.radius;
         NormalizeJob job{};
         for (int i = 0; i < tw(); ++i) {
@@ -375,6 +404,12 @@ struct vsfeel_bm3d {
         job.src_pitch = acc_pitch;
         job.out_pitch = out_pitch;
         job.out = out;
+        job.den_out = nullptr;
+        if (saved) {
+            const SavedLayout L = saved_layout();
+            job.den_out = reinterpret_cast<float*>(saved + L.den_offset) + (size_t)n * frame_floats();
+            job.den_pitch = (int)L.den_pitch;
+        }
         traced(VSFEEL_KERNEL_NORMALIZE, st, [&] { return vsfeel::launch_normalize(job, st); });
         launches += 1;
     }
@@ -382,7 +417,7 @@ struct vsfeel_bm3d {
     // Denoises outputs [first, first+count) from device frames.
     void run(const std::function<const float*(int)>& frame_ptr, int in_pitch,
              const std::function<float*(int)>& out_ptr, int out_pitch, int first, int count,
-             cudaStream_t st) {
+             cudaStream_t st, unsigned char* saved = nullptr) {
         if (count <= 0) return;
         const int r = s.radius;
         const int last = first + count - 1;
@@ -398,9 +433,10 @@ struct vsfeel_bm3d {
                 VSF_CUDA(cudaMemsetAsync(slot_pair(n, 0), 0,
                                          sizeof(float) * (size_t)tw() * 2 * acc_plane, st));
             zeroed = std::max(zeroed, want);
-            launch_stack(m, frame_ptr, in_pitch, first, last, st);
+            launch_stack(m, frame_ptr, in_pitch, first, last, st, saved);
             const int done = (m == m_hi) ? last : std::min(last, m - r);
-            for (int n = finished + 1; n <= done; ++n) launch_normalize(n, out_ptr(n), out_pitch, st);
+            for (int n = finished + 1; n <= done; ++n)
+                launch_normalize(n, out_ptr(n), out_pitch, st, saved);
             finished = std::max(finished, done);
         }
     }
@@ -617,6 +653,95 @@ int vsfeel_bm3d_process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_f
         ctx->run([&](int f) { return src + (size_t)f * src_frame_stride; }, (int)src_row_stride,
                  [&](int n) { return dst + (size_t)(n - first) * dst_frame_stride; },
                  (int)dst_row_stride, first, count, st);
+        return VSFEEL_OK;
+    });
+}
+
+int vsfeel_bm3d_saved_layout(const vsfeel_bm3d* ctx, vsfeel_bm3d_saved_info* out) {
+    if (!ctx || !out) return fail(VSFEEL_E_ARG, "null argument");
+    const auto L = ctx->saved_layout();
+    out->bytes = L.bytes;
+    out->stack_bytes = L.stack_bytes;
+    out->match_xy_offset = L.off_xy;
+    out->match_z_offset = L.off_z;
+    out->mask_offset = L.off_mask;
+    out->den_offset = L.den_offset;
+    out->den_row_stride = L.den_pitch;
+    out->den_frame_stride = (int64_t)ctx->frame_floats();
+    out->num_blocks = ctx->nblocks;
+    return VSFEEL_OK;
+}
+
+int vsfeel_bm3d_forward_saved(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
+                              int64_t src_row_stride, float* dst, int64_t dst_frame_stride,
+                              int64_t dst_row_stride, void* saved, void* stream) {
+    return guarded(ctx, [&]() -> int {
+        const Settings& s = ctx->s;
+        if (!src || !dst || !saved) return fail(VSFEEL_E_ARG, "null buffer");
+        if ((reinterpret_cast<uintptr_t>(saved) & 255u) != 0)
+            return fail(VSFEEL_E_ARG, "saved-state buffer must be 256-byte aligned");
+        if (src_row_stride < s.width || dst_row_stride < s.width || src_row_stride > INT32_MAX ||
+            dst_row_stride > INT32_MAX)
+            return fail(VSFEEL_E_ARG, "row stride smaller than the width");
+        if (src_frame_stride < src_row_stride * s.height || dst_frame_stride < dst_row_stride * s.height)
+            return fail(VSFEEL_E_ARG, "frame stride smaller than a plane");
+        cudaStream_t st = (cudaStream_t)stream;
+        ctx->run([&](int f) { return src + (size_t)f * src_frame_stride; }, (int)src_row_stride,
+                 [&](int n) { return dst + (size_t)n * dst_frame_stride; }, (int)dst_row_stride, 0,
+                 s.nframes, st, static_cast<unsigned char*>(saved));
+        return VSFEEL_OK;
+    });
+}
+
+int vsfeel_bm3d_backward(vsfeel_bm3d* ctx, const void* saved, const float* grad_out,
+                         int64_t go_frame_stride, int64_t go_row_stride, float* grad_in,
+                         int64_t gi_frame_stride, int64_t gi_row_stride, void* stream) {
+    return guarded(ctx, [&]() -> int {
+        const Settings& s = ctx->s;
+        if (!saved || !grad_out || !grad_in) return fail(VSFEEL_E_ARG, "null buffer");
+        if ((reinterpret_cast<uintptr_t>(saved) & 255u) != 0)
+            return fail(VSFEEL_E_ARG, "saved-state buffer must be 256-byte aligned");
+        if (go_row_stride < s.width || gi_row_stride < s.width || go_row_stride > INT32_MAX ||
+            gi_row_stride > INT32_MAX)
+            return fail(VSFEEL_E_ARG, "row stride smaller than the width");
+        if (go_frame_stride < go_row_stride * s.height || gi_frame_stride < gi_row_stride * s.height)
+            return fail(VSFEEL_E_ARG, "frame stride smaller than a plane");
+        cudaStream_t st = (cudaStream_t)stream;
+        const auto L = ctx->saved_layout();
+        const auto* base = static_cast<const unsigned char*>(saved);
+        // the input gradient is accumulated: clear it first (rows may be padded)
+        const size_t pitch_bytes = sizeof(float) * (size_t)gi_row_stride;
+        const size_t row_bytes = sizeof(float) * (size_t)s.width;
+        if (gi_frame_stride == gi_row_stride * s.height) {
+            VSF_CUDA(cudaMemset2DAsync(grad_in, pitch_bytes, 0, row_bytes,
+                                       (size_t)s.height * s.nframes, st));
+        } else {
+            for (int f = 0; f < s.nframes; ++f)
+                VSF_CUDA(cudaMemset2DAsync(grad_in + (size_t)f * gi_frame_stride, pitch_bytes, 0,
+                                           row_bytes, (size_t)s.height, st));
+        }
+        AdjointJob job{};
+        job.saved = base;
+        job.stack_bytes = L.stack_bytes;
+        job.off_xy = L.off_xy;
+        job.off_z = L.off_z;
+        job.off_mask = L.off_mask;
+        job.den = reinterpret_cast<const float*>(base + L.den_offset);
+        job.den_frame = (int64_t)ctx->frame_floats();
+        job.den_pitch = (int)L.den_pitch;
+        job.grad_out = grad_out;
+        job.go_frame = go_frame_stride;
+        job.go_pitch = (int)go_row_stride;
+        job.grad_in = grad_in;
+        job.gi_frame = gi_frame_stride;
+        job.gi_pitch = (int)gi_row_stride;
+        job.nframes = s.nframes;
+        job.radius = s.radius;
+        job.nblocks = ctx->nblocks;
+        job.width = s.width;
+        job.height = s.height;
+        ctx->traced(VSFEEL_KERNEL_ADJOINT, st, [&] { return launch_adjoint(job, st); });
+        ctx->launches += 1;
         return VSFEEL_OK;
     });
 }

@@ -314,6 +314,10 @@ __device__ __forceinline__ void transform_group_axis(float d[64], bool inverse) 
 
 }  // namespace
 
+// kSaveMask: also record the keep bits of every coefficient, lane `sub`
+// writing word mask_out[block * 8 + sub] (bit 8 * group_freq + vertical_freq
+// of horizontal frequency `sub`), for the adjoint.
+template <bool kSaveMask>
 __global__ void __launch_bounds__(128) bm3d_filter_kernel(const StackJob job) {
     __shared__ float smem[kGroupsPerCta / 4 * 4 * kGroupStride];
     const int lane = threadIdx.x & 31;
@@ -350,13 +354,16 @@ __global__ void __launch_bounds__(128) bm3d_filter_kernel(const StackJob job) {
 
     const float thr = job.thr;
     int kept = 0;
+    uint64_t bits = 0;
 #pragma unroll
     for (int i = 0; i < 64; ++i) {
         const float t = (i == 0 && sub == 0) ? 0.0f : thr;
         const bool keep = fabsf(d[i]) >= t;
         kept += keep ? 1 : 0;
+        if (kSaveMask) bits |= keep ? (uint64_t(1) << i) : uint64_t(0);
         d[i] = keep ? __fmul_rn(d[i], 1.0f / 4096.0f) : 0.0f;
     }
+    if (kSaveMask && valid) job.mask_out[(size_t)b * 8 + sub] = bits;
     kept += __shfl_xor_sync(kFull, kept, 1);
     kept += __shfl_xor_sync(kFull, kept, 2);
     kept += __shfl_xor_sync(kFull, kept, 4);
@@ -400,6 +407,99 @@ __global__ void __launch_bounds__(256) bm3d_normalize_kernel(const NormalizeJob 
         acw += (double)job.num[i][o + job.den_offset];
     }
     job.out[(size_t)y * job.out_pitch + x] = (float)(acc / acw);
+    if (job.den_out) job.den_out[(size_t)y * job.den_pitch + x] = (float)acw;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint of the frozen-match operator (no counterpart in the reference).
+//
+// With the match table, the keep bits and so the weights w = 1/kept frozen,
+// the forward pass is linear in the input: every group adds
+// w * S^T (F^-1 M F / 4096) S x to its slices, S gathering the 8 matched
+// patches, F the scaled 3D DCT and M the keep mask, and output n divides the
+// sum of the slices it reads by the frozen denominator D_n. F^-1 is F^T up
+// to the same scale, so F^-1 M F / 4096 is symmetric and the adjoint of a
+// group is the same transform, mask and inverse applied to the gathered
+// output gradient. Per group: gather reads(m, z) * g / D from the output
+// gradient of each patch's frame, transform, mask, inverse, times w, then
+// scatter-add into the input gradient of the same patches. The extractor's
+// rounding of the forward scatter is taken as the identity.
+__global__ void __launch_bounds__(128) bm3d_adjoint_kernel(const AdjointJob job) {
+    __shared__ float smem[kGroupsPerCta / 4 * 4 * kGroupStride];
+    const int lane = threadIdx.x & 31;
+    const int sub = lane & 7;
+    const int group_in_cta = threadIdx.x >> 3;
+    float* buf = smem + group_in_cta * kGroupStride;
+    const int64_t total = (int64_t)job.nframes * job.nblocks;
+    const int64_t gid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 3;
+    const bool valid = gid < total;
+    const int64_t g = valid ? gid : total - 1;
+    const int m = (int)(g / job.nblocks);
+    const int b = (int)(g - (int64_t)m * job.nblocks);
+    const unsigned char* rec = job.saved + (size_t)m * job.stack_bytes;
+
+    const uint4* xy4 = reinterpret_cast<const uint4*>(rec + job.off_xy) + (size_t)b * 2;
+    const uint4 m0 = xy4[0], m1 = xy4[1];
+    uint32_t mxy[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+    // a damaged state must not send the gathers outside the frames
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t x = min(mxy[k] & 0xffffu, (uint32_t)(job.width - 8));
+        const uint32_t y = min(mxy[k] >> 16, (uint32_t)(job.height - 8));
+        mxy[k] = x | (y << 16);
+    }
+    const uint32_t zp = reinterpret_cast<const uint32_t*>(rec + job.off_z)[b];
+    const uint64_t bits = reinterpret_cast<const uint64_t*>(rec + job.off_mask)[(size_t)b * 8 + sub];
+    const int r = job.radius;
+
+    float d[64];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int z = (int)((zp >> (4 * k)) & 15u);
+        const int f = clamp_frame(m - r + z, job.nframes);
+        const float reads = (float)slice_reads(m, z, job.nframes, r);
+        const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
+        const float* go = job.grad_out + (size_t)f * job.go_frame + (size_t)my * job.go_pitch + mx + sub;
+        const float* dn = job.den + (size_t)f * job.den_frame + (size_t)my * job.den_pitch + mx + sub;
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            d[k * 8 + j] = reads == 0.0f
+                               ? 0.0f
+                               : __fdiv_rn(__fmul_rn(reads, __ldg(go + (size_t)j * job.go_pitch)),
+                                           __ldg(dn + (size_t)j * job.den_pitch));
+    }
+
+    transform_rows(d, false);
+    transpose_group(d, buf, sub);
+    transform_rows(d, false);
+    transpose_group(d, buf, sub);
+    transform_group_axis(d, false);
+
+    int kept = __popcll(bits);
+    kept += __shfl_xor_sync(kFull, kept, 1);
+    kept += __shfl_xor_sync(kFull, kept, 2);
+    kept += __shfl_xor_sync(kFull, kept, 4);
+    const float w = __fdiv_rn(1.0f, (float)max(kept, 1));
+#pragma unroll
+    for (int i = 0; i < 64; ++i)
+        d[i] = ((bits >> i) & 1u) ? __fmul_rn(d[i], 1.0f / 4096.0f) : 0.0f;
+
+    transform_rows(d, true);
+    transpose_group(d, buf, sub);
+    transform_rows(d, true);
+    transpose_group(d, buf, sub);
+    transform_group_axis(d, true);
+
+    if (!valid) return;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int z = (int)((zp >> (4 * k)) & 15u);
+        const int f = clamp_frame(m - r + z, job.nframes);
+        const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
+        float* gi = job.grad_in + (size_t)f * job.gi_frame + (size_t)my * job.gi_pitch + mx + sub;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) atomicAdd(gi + (size_t)j * job.gi_pitch, __fmul_rn(w, d[k * 8 + j]));
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -419,7 +519,19 @@ cudaError_t launch_match(const StackJob& job, cudaStream_t stream) {
 }
 
 cudaError_t launch_filter(const StackJob& job, cudaStream_t stream) {
-    bm3d_filter_kernel<<<block_grid(job), kThreads, 0, stream>>>(job);
+    if (job.mask_out)
+        bm3d_filter_kernel<true><<<block_grid(job), kThreads, 0, stream>>>(job);
+    else
+        bm3d_filter_kernel<false><<<block_grid(job), kThreads, 0, stream>>>(job);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream) {
+    const int64_t threads = (int64_t)job.nframes * job.nblocks * 8;
+    const int64_t grid = (threads + kThreads - 1) / kThreads;
+    if (grid <= 0) return cudaSuccess;
+    if (grid > INT32_MAX) return cudaErrorInvalidValue;
+    bm3d_adjoint_kernel<<<(unsigned)grid, kThreads, 0, stream>>>(job);
     return cudaGetLastError();
 }
 

@@ -28,6 +28,9 @@ EXPORTS = (
     "vsfeel_bm3d_launch_count",
     "vsfeel_bm3d_trace",
     "vsfeel_bm3d_trace_read",
+    "vsfeel_bm3d_saved_layout",
+    "vsfeel_bm3d_forward_saved",
+    "vsfeel_bm3d_backward",
     "vsfeel_bm3d_process_device_noalloc",
     "vsfeel_bm3d_noalloc_scratch_bytes",
     "vsfeel_bm3d_last_error",
@@ -48,8 +51,10 @@ E_UNSUPPORTED = -7
 KERNEL_MATCH = 0
 KERNEL_FILTER = 1
 KERNEL_NORMALIZE = 2
-KERNEL_KINDS = 3
-KERNEL_NAMES = ("bm3d_match_kernel", "bm3d_filter_kernel", "bm3d_normalize_kernel")
+KERNEL_ADJOINT = 3
+KERNEL_KINDS = 4
+KERNEL_NAMES = ("bm3d_match_kernel", "bm3d_filter_kernel", "bm3d_normalize_kernel",
+                "bm3d_adjoint_kernel")
 
 CF_GRAY = 1
 CF_YUV = 3
@@ -94,6 +99,12 @@ class Info(ctypes.Structure):
         ("blocks_x", ctypes.c_int), ("blocks_y", ctypes.c_int),
         ("device_bytes", ctypes.c_int64),
     ]
+
+
+class SavedInfo(ctypes.Structure):
+    _fields_ = [(name, ctypes.c_int64) for name in (
+        "bytes", "stack_bytes", "match_xy_offset", "match_z_offset", "mask_offset",
+        "den_offset", "den_row_stride", "den_frame_stride", "num_blocks")]
 
 
 FETCH_FN = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
@@ -142,6 +153,12 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.vsfeel_bm3d_trace_read.argtypes = [c_p, ctypes.POINTER(ctypes.c_double),
                                            ctypes.POINTER(c_i64)]
     lib.vsfeel_bm3d_trace_read.restype = c_int
+    lib.vsfeel_bm3d_saved_layout.argtypes = [c_p, ctypes.POINTER(SavedInfo)]
+    lib.vsfeel_bm3d_saved_layout.restype = c_int
+    lib.vsfeel_bm3d_forward_saved.argtypes = [c_p, c_p, c_i64, c_i64, c_p, c_i64, c_i64, c_p, c_p]
+    lib.vsfeel_bm3d_forward_saved.restype = c_int
+    lib.vsfeel_bm3d_backward.argtypes = [c_p, c_p, c_p, c_i64, c_i64, c_p, c_i64, c_i64, c_p]
+    lib.vsfeel_bm3d_backward.restype = c_int
     lib.vsfeel_bm3d_process_device_noalloc.argtypes = [ctypes.POINTER(Args),
                                                        ctypes.POINTER(VideoInfo), c_p, c_i64,
                                                        c_i64, c_p, c_i64, c_i64, c_int, c_int, c_p]
