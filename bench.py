@@ -222,6 +222,81 @@ def time_fwd_bwd(torch, dev, name, steps, warmup):
             "steps": steps, "warmup": warmup}
 
 
+def batched_clips(rng):
+    """The batched workload: 64 clips of 16 frames, 16 at 640x360, 24 at
+    1280x720, 16 at 1920x1080 and 8 at 3840x2160; per clip sigma U[1, 10],
+    radius from {0, 1, 2}, block_step from {4, 8}; bm_range 16, ps_num 2,
+    ps_range 7."""
+    sizes = [(640, 360)] * 16 + [(1280, 720)] * 24 + [(1920, 1080)] * 16 + [(3840, 2160)] * 8
+    out = []
+    for i, (w, h) in enumerate(sizes):
+        params = dict(sigma=float(rng.uniform(1.0, 10.0)), block_step=int(rng.choice([4, 8])),
+                      bm_range=16, radius=int(rng.choice([0, 1, 2])), ps_num=2, ps_range=7)
+        out.append((16, h, w, params))
+    return out
+
+
+def time_batched(torch, dev, steps, warmup):
+    """The batched form on the 64-clip workload, against the same clips run
+    one after another through the plain path (device-resident, CUDA events)."""
+    import numpy as np
+
+    from vsfeel.autograd import Denoiser
+    from vsfeel.batch import Batch
+    from vsfeel.synthetic import make_clip_device
+
+    spec = batched_clips(np.random.default_rng(3000))
+    src, dst = [], []
+    for i, (n, h, w, p) in enumerate(spec):
+        src.append(make_clip_device(n, h, w, p["sigma"], shift=4, seed=3000 + i, device=dev))
+        dst.append(torch.empty_like(src[-1]))
+    px = sum(n * h * w for n, h, w, _ in spec)
+    t0 = time.perf_counter()
+    batch = Batch([(s, d, p) for s, d, (_, _, _, p) in zip(src, dst, spec)], device=dev.index,
+                  autotune=True)
+    create_s = time.perf_counter() - t0
+    for _ in range(warmup):
+        batch.run()
+    torch.cuda.synchronize()
+    batch.finish()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        batch.run()
+    b.record()
+    torch.cuda.synchronize()
+    batch.finish()
+    batched_ms = a.elapsed_time(b) / steps
+    classes = batch.classes()
+    device_bytes = batch.device_bytes
+    batched_out = [d.clone() for d in dst[:4]]
+    batch.close()
+
+    # the plain path, clip after clip, each at its steady state
+    plain_ms = 0.0
+    worst = 0.0
+    for i, (s, d, (n, h, w, p)) in enumerate(zip(src, dst, spec)):
+        den = Denoiser(s.shape, dev.index, **p)
+        den.plain(s, d)
+        torch.cuda.synchronize()
+        a.record()
+        for _ in range(2):
+            den.plain(s, d)
+        b.record()
+        torch.cuda.synchronize()
+        plain_ms += a.elapsed_time(b) / 2
+        if i < 4:
+            worst = max(worst, float((d - batched_out[i]).abs().max()))
+        den.close()
+    return {"workload": "batched_64_clips_mixed_360p_to_2160p_x16_frames",
+            "batched_mpx_s": px / batched_ms / 1e3, "batched_ms": batched_ms,
+            "plain_sequential_mpx_s": px / plain_ms / 1e3, "plain_sequential_ms": plain_ms,
+            "batched_over_plain_sequential": plain_ms / batched_ms,
+            "megapixels_per_step": px / 1e6, "create_and_autotune_s": create_s,
+            "classes": classes, "device_bytes": device_bytes,
+            "max_abs_diff_vs_plain_first4": worst, "steps": steps, "warmup": warmup}
+
+
 def run_reference(args) -> int:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -289,6 +364,7 @@ def main() -> int:
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer pass")
     ap.add_argument("--no-grad", action="store_true",
                     help="skip the forward+backward measurements")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
@@ -410,6 +486,8 @@ def main() -> int:
     if world == 1 and not args.no_grad:
         line["fwd_bwd"] = [time_fwd_bwd(torch, dev, name, max(3, args.steps // 2), 3)
                            for name in GRAD_WORKLOADS]
+    if world == 1 and not args.no_batch:
+        line["batched"] = time_batched(torch, dev, max(2, args.steps // 3), 3)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(luma)
     print(json.dumps(line), flush=True)

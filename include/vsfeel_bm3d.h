@@ -201,6 +201,72 @@ VSFEEL_API int vsfeel_bm3d_backward(vsfeel_bm3d* ctx, const void* saved, const f
                                     int64_t go_frame_stride, int64_t go_row_stride, float* grad_in,
                                     int64_t gi_frame_stride, int64_t gi_row_stride, void* stream);
 
+/* ---- Batched form (no counterpart in the reference) -----------------------
+ *
+ * Many clips of uneven sizes and settings denoised together; this replaces
+ * the reference's num_streams concurrency. Clips are grouped into shape
+ * classes (equal radius, block_step, bm_range, ps_num and ps_range). Per
+ * class, one persistent launch works through a device queue of
+ * (stack, tile) items of all the class's clips, matching each tile, one
+ * launch filters every block of every stack and one normalises all the
+ * class's output frames; the class's work is captured once in a CUDA graph. Classes run concurrently. With
+ * VSFEEL_BATCH_AUTOTUNE, vsfeel_bm3d_batch_create times every tile shape
+ * that fits a class on one of its stacks and keeps the fastest; otherwise
+ * the largest fitting shape is used. A class that no shape fits (radius >= 3,
+ * or windows too large) runs the direct-read kernels stack by stack inside
+ * its graph.
+ *
+ * Buffers are bound at creation: every vsfeel_bm3d_batch_run replays the
+ * graphs on the same src/dst buffers (device memory, strides in floats), so
+ * new input goes into the same src buffers. Each clip is a GRAYS 32-bit
+ * float clip; its outputs are all its frames. */
+typedef struct vsfeel_bm3d_batch_clip {
+    vsfeel_bm3d_args args;          /* per clip; "ref" is not supported   */
+    int width, height, num_frames;
+    const float* src;
+    int64_t src_frame_stride, src_row_stride;
+    float* dst;
+    int64_t dst_frame_stride, dst_row_stride;
+} vsfeel_bm3d_batch_clip;
+
+typedef struct vsfeel_bm3d_batch vsfeel_bm3d_batch;
+
+enum { VSFEEL_BATCH_AUTOTUNE = 1 };
+/* flags: use tile shape s for every class it fits (tests and tuning runs) */
+#define VSFEEL_BATCH_FORCE_SHAPE(s) ((((s) + 1) & 15) << 4)
+
+/* Tile shapes of the tiled matcher, in reference blocks (x by y). */
+enum { VSFEEL_TILE_8X4 = 0, VSFEEL_TILE_16X2 = 1, VSFEEL_TILE_4X8 = 2, VSFEEL_TILE_8X2 = 3,
+       VSFEEL_TILE_4X4 = 4, VSFEEL_TILE_SHAPES = 5 };
+
+typedef struct vsfeel_bm3d_batch_class_info {
+    int radius, block_step, bm_range, ps_num, ps_range;
+    int clips, stacks;
+    int64_t tiles;          /* work-queue items per run                      */
+    int tile_shape;         /* VSFEEL_TILE_*, or -1: direct-read kernels     */
+    double tuned_ms[VSFEEL_TILE_SHAPES]; /* autotuner's time per shape, or 0 */
+} vsfeel_bm3d_batch_class_info;
+
+VSFEEL_API int vsfeel_bm3d_batch_create(const vsfeel_bm3d_batch_clip* clips, int nclips, int device,
+                                        int flags, vsfeel_bm3d_batch** out);
+
+/* Enqueues one denoising of every clip, ordered after the work already on
+ * `stream` (used as given); the call returns once the work is enqueued and
+ * later work on `stream` waits for it. */
+VSFEEL_API int vsfeel_bm3d_batch_run(vsfeel_bm3d_batch* batch, void* stream);
+
+/* Waits (bounded) for the batch's enqueued work and reports an internal
+ * error the kernels flagged. */
+VSFEEL_API int vsfeel_bm3d_batch_finish(vsfeel_bm3d_batch* batch);
+
+VSFEEL_API int vsfeel_bm3d_batch_classes(const vsfeel_bm3d_batch* batch, int* nclasses,
+                                         int64_t* device_bytes);
+VSFEEL_API int vsfeel_bm3d_batch_class(const vsfeel_bm3d_batch* batch, int index,
+                                       vsfeel_bm3d_batch_class_info* info);
+
+/* Frees the batch (waits, bounded, for its work first). Accepts NULL. */
+VSFEEL_API void vsfeel_bm3d_batch_free(vsfeel_bm3d_batch* batch);
+
 /* Allocation-free form of vsfeel_bm3d_process_device; it has no counterpart
  * in the reference. It is for callers that cannot let this library allocate
  * device memory: processes that reserve the GPU's memory in their own fixed

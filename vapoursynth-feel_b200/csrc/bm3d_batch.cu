@@ -1,0 +1,593 @@
+// Batched form: many clips of uneven sizes and settings in one run (the
+// vsfeel_bm3d_batch_* entry points of include/vsfeel_bm3d.h). It has no
+// counterpart in the reference, whose concurrency is num_streams Vulkan
+// queues working on frames of one clip (src/bm3d.cpp:698-1028).
+//
+// Layout. Every clip keeps, per output frame n, the TW (numerator, weight)
+// plane pairs of its contributing stacks (the plain path's slot, without
+// the ring reuse): all stacks of all clips can then be in flight at once.
+// Shape classes group the clips whose stacks share a tiled-kernel
+// configuration. Per class:
+//   * jobs[]: one StackJob per (clip, stack), largest clips first, with the
+//     prefix sums of their tile counts -- the persistent kernel's queue;
+//   * norm[]: one NormalizeJob per output frame, with the prefix sums of
+//     their 32x8 tiles;
+//   * a match table per stack;
+//   * a CUDA graph: clear the class's accumulators and queue counter, the
+//     persistent matching launch (one CTA per SM) over the queue, one filter
+//     launch over every block of every stack, one normalise launch. (The
+//     filter stays a separate kernel: inside the matcher's one CTA per SM
+//     its atomics run slower than at the filter kernel's occupancy.)
+//     Classes whose stacks no tile shape fits record the direct-read match
+//     and filter kernels per stack instead.
+// A run forks the caller's stream into one stream per class, replays the
+// graphs and joins back.
+#include "bm3d_device.cuh"
+#include "vsfeel_bm3d.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <functional>
+#include <map>
+#include <string>
+#include <thread>
+#include <tuple>
+#include <vector>
+
+namespace vsfeel {
+int parse_to_info(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
+                  vsfeel_bm3d_info* info);
+int set_error(int code, const char* msg);
+}  // namespace vsfeel
+
+namespace {
+
+using namespace vsfeel;
+
+int error(int code, const std::string& msg) { return set_error(code, msg.c_str()); }
+
+struct Fail {
+    int code;
+    std::string msg;
+};
+
+void check(cudaError_t e, const char* what) {
+    if (e == cudaSuccess) return;
+    cudaGetLastError();
+    if (e == cudaErrorMemoryAllocation)
+        throw Fail{VSFEEL_E_MEMORY, std::string("out of device memory (") + what + ")"};
+    throw Fail{VSFEEL_E_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e) + " (" + what + ")"};
+}
+
+int64_t timeout_ms() {
+    const char* s = std::getenv("VSFEEL_TIMEOUT_MS");
+    if (s && *s) {
+        const long long v = std::atoll(s);
+        if (v > 0) return v;
+    }
+    return 120000;
+}
+
+// Bounded wait for a stream.
+int wait_stream(cudaStream_t s) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const int64_t limit = timeout_ms();
+    for (int spins = 0;; ++spins) {
+        const cudaError_t e = cudaStreamQuery(s);
+        if (e == cudaSuccess) return VSFEEL_OK;
+        if (e != cudaErrorNotReady)
+            return error(VSFEEL_E_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+        const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                            std::chrono::steady_clock::now() - t0)
+                            .count();
+        if (ms >= limit)
+            return error(VSFEEL_E_TIMEOUT,
+                         "timed out after " + std::to_string(ms) + " ms waiting for the GPU");
+        if (spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+template <class T>
+struct Dev {
+    T* p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count) {
+        release();
+        if (count == 0) return;
+        check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+        n = count;
+    }
+    void upload(const std::vector<T>& v) {
+        alloc(v.size());
+        if (!v.empty()) check(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice),
+                              "cudaMemcpy");
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+inline int clampi(int v, int lo, int hi) { return std::min(std::max(v, lo), hi); }
+
+struct Clip {
+    vsfeel_bm3d_batch_clip desc;
+    vsfeel_bm3d_info info;
+    int acc_pitch = 0;
+    size_t plane = 0;      // floats per accumulator plane
+    size_t acc_off = 0;    // floats from the class's accumulator base
+    int tw() const { return 2 * info.radius + 1; }
+    size_t acc_floats() const { return (size_t)info.num_frames * tw() * 2 * plane; }
+};
+
+using ClassKey = std::tuple<int, int, int, int, int>;  // radius, step, R, P, Q
+
+struct Class {
+    ClassKey key;
+    std::vector<int> clips;
+    std::vector<StackJob> jobs;
+    int tile_shape = -1;
+    double tuned_ms[kTileShapes] = {};
+    int64_t tiles = 0;
+    size_t smem = 0;
+    Dev<StackJob> d_jobs;
+    Dev<int> d_tile_first;
+    Dev<NormalizeJob> d_norm;
+    Dev<int> d_norm_first;
+    int norm_tiles = 0;
+    int nnorm = 0;
+    Dev<float> acc;
+    Dev<uint32_t> match_xy, match_z;  // match tables (one per stack, or one shared)
+    Dev<int> d_filter_first;
+    int filter_items = 0;
+    Dev<int> counter;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+}  // namespace
+
+struct vsfeel_bm3d_batch {
+    int device = 0;
+    int sms = 0;
+    std::vector<Clip> clips;
+    std::vector<Class> classes;
+    Dev<int> status;
+    cudaEvent_t start = nullptr;
+    int64_t device_bytes = 0;
+
+    ~vsfeel_bm3d_batch() {
+        for (Class& c : classes) {
+            if (c.stream) wait_stream(c.stream);
+            if (c.exec) cudaGraphExecDestroy(c.exec);
+            if (c.graph) cudaGraphDestroy(c.graph);
+            if (c.done) cudaEventDestroy(c.done);
+            if (c.stream) cudaStreamDestroy(c.stream);
+            c.d_jobs.release();
+            c.d_tile_first.release();
+            c.d_norm.release();
+            c.d_norm_first.release();
+            c.acc.release();
+            c.match_xy.release();
+            c.match_z.release();
+            c.d_filter_first.release();
+            c.counter.release();
+        }
+        if (start) cudaEventDestroy(start);
+        status.release();
+    }
+
+    // The StackJob of stack m of clip c, scattering into the class's
+    // accumulators (slice_dst null when `silent`).
+    StackJob make_job(const Clip& c, float* acc_base, int m, bool silent) const {
+        const vsfeel_bm3d_info& in = c.info;
+        const int r = in.radius, N = in.num_frames, tw = c.tw();
+        StackJob job{};
+        for (int z = 0; z < tw; ++z) {
+            const int n = clampi(m - r + z, 0, N - 1);
+            job.slice_frame[z] = c.desc.src + (size_t)n * c.desc.src_frame_stride;
+            job.slice_dst[z] = nullptr;
+            if (silent || slice_reads(m, z, N, r) == 0) continue;
+            const int j = m - (n - r);
+            job.slice_dst[z] = acc_base + c.acc_off + ((size_t)n * tw + j) * 2 * c.plane;
+        }
+        job.dst_plane = (int64_t)c.plane;
+        job.pitch = (int)c.desc.src_row_stride;
+        job.dst_pitch = c.acc_pitch;
+        job.width = in.width;
+        job.height = in.height;
+        job.radius = r;
+        job.step = in.block_step;
+        job.bm_range = in.bm_range;
+        job.ps_num = in.ps_num;
+        job.ps_range = in.ps_range;
+        job.nbx = in.blocks_x;
+        job.nby = in.blocks_y;
+        job.thr = in.threshold;
+        job.extractor = in.extractor;
+        job.status = status.p;
+        return job;
+    }
+};
+
+namespace {
+
+// Times every fitting tile shape on one stack of the class (no scatter) and
+// returns the fastest.
+int autotune(vsfeel_bm3d_batch* b, Class& cls, const StackJob& sample_in, const bool fits[]) {
+    // the sample writes its match table into scratch of its own
+    StackJob sample = sample_in;
+    Dev<uint32_t> xy, zz;
+    xy.alloc((size_t)sample.nbx * sample.nby * 8);
+    zz.alloc((size_t)sample.nbx * sample.nby);
+    sample.match_xy = xy.p;
+    sample.match_z = zz.p;
+    Dev<StackJob> job;
+    job.upload(std::vector<StackJob>{sample});
+    Dev<int> first, counter;
+    first.alloc(2);
+    counter.alloc(1);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    struct Cleanup {  // frees the tuning scratch on every exit
+        std::function<void()> fn;
+        ~Cleanup() { fn(); }
+    } cleanup{[&] {
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+        xy.release();
+        zz.release();
+        job.release();
+        first.release();
+        counter.release();
+    }};
+    check(cudaEventCreate(&e0), "cudaEventCreate");
+    check(cudaEventCreate(&e1), "cudaEventCreate");
+    int best = -1;
+    double best_ms = 0.0;
+    for (int s = 0; s < kTileShapes; ++s) {
+        if (!fits[s]) continue;
+        const int tiles = tile_count(sample, TileShape(s));
+        const int h_first[2] = {0, tiles};
+        check(cudaMemcpy(first.p, h_first, sizeof(h_first), cudaMemcpyHostToDevice), "cudaMemcpy");
+        const size_t smem = tile_smem_bytes(sample, TileShape(s), kTableOnly);
+        const BatchWork work{job.p, first.p, 1, counter.p};
+        const int grid = std::min(b->sms, tiles);
+        float best_rep = 0.0f;
+        for (int rep = 0; rep < 4; ++rep) {
+            check(cudaMemsetAsync(counter.p, 0, sizeof(int), cls.stream), "cudaMemsetAsync");
+            check(cudaEventRecord(e0, cls.stream), "cudaEventRecord");
+            check(launch_batch_tiles(work, TileShape(s), kTableOnly, smem, grid, cls.stream),
+                  "autotune launch");
+            check(cudaEventRecord(e1, cls.stream), "cudaEventRecord");
+            if (wait_stream(cls.stream) != VSFEEL_OK)
+                throw Fail{VSFEEL_E_TIMEOUT, "timed out while autotuning"};
+            float ms = 0.0f;
+            check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+            if (rep > 0 && (rep == 1 || ms < best_rep)) best_rep = ms;  // first run warms up
+        }
+        cls.tuned_ms[s] = best_rep;
+        if (best < 0 || best_rep < best_ms) {
+            best = s;
+            best_ms = best_rep;
+        }
+    }
+    return best;
+}
+
+void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
+    check(cudaStreamCreateWithFlags(&cls.stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaEventCreateWithFlags(&cls.done, cudaEventDisableTiming), "cudaEventCreate");
+    // largest clips first: the queue's tail is made of small tiles
+    std::stable_sort(cls.clips.begin(), cls.clips.end(), [&](int a, int c) {
+        const auto& A = b->clips[a].info;
+        const auto& C = b->clips[c].info;
+        return (int64_t)A.width * A.height > (int64_t)C.width * C.height;
+    });
+    size_t acc_floats = 0;
+    for (int ci : cls.clips) {
+        Clip& c = b->clips[ci];
+        c.acc_off = acc_floats;
+        acc_floats += (c.acc_floats() + 63) & ~size_t(63);
+    }
+    cls.acc.alloc(acc_floats);
+    cls.counter.alloc(1);
+    b->device_bytes += (int64_t)acc_floats * 4;
+
+    // which tile shapes fit every stack of the class
+    bool fits[kTileShapes];
+    for (int s = 0; s < kTileShapes; ++s) fits[s] = true;
+    size_t max_nblocks = 0;
+    for (int ci : cls.clips) {
+        const Clip& c = b->clips[ci];
+        const StackJob probe = b->make_job(c, cls.acc.p, 0, true);
+        for (int s = 0; s < kTileShapes; ++s)
+            fits[s] = fits[s] && tile_shape_fits(probe, TileShape(s), kTableOnly);
+        max_nblocks = std::max(max_nblocks, (size_t)c.info.blocks_x * c.info.blocks_y);
+    }
+    int shape = -1;
+    if (forced >= 0 && forced < kTileShapes && fits[forced]) {
+        shape = forced;
+    } else if (tune) {
+        const Clip& big = b->clips[cls.clips.front()];
+        const StackJob sample = b->make_job(big, cls.acc.p, big.info.num_frames / 2, true);
+        bool any = false;
+        for (int s = 0; s < kTileShapes; ++s) any = any || fits[s];
+        if (any) shape = autotune(b, cls, sample, fits);
+    } else {
+        const TileShape order[] = {kTile8x4, kTile16x2, kTile8x2, kTile4x4};
+        for (TileShape s : order)
+            if (fits[s]) {
+                shape = s;
+                break;
+            }
+    }
+    cls.tile_shape = shape;
+
+    // queue of (stack, tile) items and the normalisation list
+    std::vector<int> first{0}, nfirst{0}, ffirst{0};
+    std::vector<NormalizeJob> norm;
+    for (int ci : cls.clips) {
+        const Clip& c = b->clips[ci];
+        const int N = c.info.num_frames, r = c.info.radius, tw = c.tw();
+        for (int m = 0; m < N; ++m) {
+            StackJob job = b->make_job(c, cls.acc.p, m, false);
+            if (shape >= 0) {
+                cls.smem = std::max(cls.smem, tile_smem_bytes(job, TileShape(shape), kTableOnly));
+                first.push_back(first.back() + tile_count(job, TileShape(shape)));
+                const int64_t fi = (int64_t)ffirst.back() + filter_items(c.info.blocks_x * c.info.blocks_y);
+                if (fi > INT32_MAX) throw Fail{VSFEEL_E_ARG, "batch too large for one filter launch"};
+                ffirst.push_back((int)fi);
+            }
+            cls.jobs.push_back(job);
+        }
+        for (int n = 0; n < N; ++n) {
+            NormalizeJob nj{};
+            for (int i = 0; i < tw; ++i) {
+                const int m = clampi(n - r + i, 0, N - 1);
+                nj.num[i] = cls.acc.p + c.acc_off + ((size_t)n * tw + (m - (n - r))) * 2 * c.plane;
+            }
+            nj.den_offset = (int64_t)c.plane;
+            nj.tw = tw;
+            nj.width = c.info.width;
+            nj.height = c.info.height;
+            nj.src_pitch = c.acc_pitch;
+            nj.out_pitch = (int)c.desc.dst_row_stride;
+            nj.out = c.desc.dst + (size_t)n * c.desc.dst_frame_stride;
+            norm.push_back(nj);
+            const int64_t nt = (int64_t)nfirst.back() + normalize_tiles(nj.width, nj.height);
+            if (nt > INT32_MAX) throw Fail{VSFEEL_E_ARG, "batch too large for one normalise launch"};
+            nfirst.push_back((int)nt);
+        }
+    }
+    if (shape >= 0 && first.back() < 0) throw Fail{VSFEEL_E_ARG, "batch too large for one queue"};
+    cls.tiles = shape >= 0 ? first.back() : 0;
+    if (shape < 0) {
+        // direct-read kernels, stack after stack: one match table suffices
+        cls.match_xy.alloc(max_nblocks * 8);
+        cls.match_z.alloc(max_nblocks);
+        for (StackJob& j : cls.jobs) {
+            j.match_xy = cls.match_xy.p;
+            j.match_z = cls.match_z.p;
+        }
+    } else {
+        // every stack is in flight at once: one match table each
+        size_t total = 0;
+        for (const StackJob& j : cls.jobs) total += (size_t)j.nbx * j.nby;
+        cls.match_xy.alloc(total * 8);
+        cls.match_z.alloc(total);
+        size_t off = 0;
+        for (StackJob& j : cls.jobs) {
+            j.match_xy = cls.match_xy.p + off * 8;
+            j.match_z = cls.match_z.p + off;
+            off += (size_t)j.nbx * j.nby;
+        }
+        cls.d_filter_first.upload(ffirst);
+        cls.filter_items = ffirst.back();
+    }
+    cls.d_jobs.upload(cls.jobs);
+    if (shape >= 0) cls.d_tile_first.upload(first);
+    cls.d_norm.upload(norm);
+    cls.d_norm_first.upload(nfirst);
+    cls.nnorm = (int)norm.size();
+    cls.norm_tiles = nfirst.back();
+    b->device_bytes += (int64_t)(cls.match_xy.n + cls.match_z.n) * 4;
+
+    // capture the class's run
+    check(cudaStreamBeginCapture(cls.stream, cudaStreamCaptureModeRelaxed), "capture");
+    cudaError_t err = cudaMemsetAsync(cls.acc.p, 0, acc_floats * sizeof(float), cls.stream);
+    if (err == cudaSuccess && shape >= 0) {
+        err = cudaMemsetAsync(cls.counter.p, 0, sizeof(int), cls.stream);
+        const BatchWork work{cls.d_jobs.p, cls.d_tile_first.p, (int)cls.jobs.size(), cls.counter.p};
+        const int grid = (int)std::min<int64_t>(b->sms, cls.tiles);
+        if (err == cudaSuccess)
+            err = launch_batch_tiles(work, TileShape(shape), kTableOnly, cls.smem, grid, cls.stream);
+        const FilterBatch fw{cls.d_jobs.p, cls.d_filter_first.p, (int)cls.jobs.size()};
+        if (err == cudaSuccess) err = launch_filter_batch(fw, cls.filter_items, cls.stream);
+    } else if (err == cudaSuccess) {
+        for (const StackJob& j : cls.jobs) {
+            err = launch_match(j, cls.stream);
+            if (err == cudaSuccess) err = launch_filter(j, cls.stream);
+            if (err != cudaSuccess) break;
+        }
+    }
+    if (err == cudaSuccess) {
+        const NormalizeBatch nw{cls.d_norm.p, cls.d_norm_first.p, cls.nnorm};
+        err = launch_normalize_batch(nw, cls.norm_tiles, cls.stream);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(cls.stream, &graph);
+    cls.graph = graph;
+    check(err, "recording the class's graph");
+    check(end, "cudaStreamEndCapture");
+    check(cudaGraphInstantiate(&cls.exec, cls.graph, 0), "cudaGraphInstantiate");
+}
+
+}  // namespace
+
+extern "C" {
+
+int vsfeel_bm3d_batch_create(const vsfeel_bm3d_batch_clip* clips, int nclips, int device, int flags,
+                             vsfeel_bm3d_batch** out) {
+    if (!out) return error(VSFEEL_E_ARG, "null output pointer");
+    *out = nullptr;
+    if (!clips || nclips <= 0) return error(VSFEEL_E_ARG, "no clips");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return error(VSFEEL_E_CUDA, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return error(VSFEEL_E_ARG, "invalid device ordinal");
+
+    auto* b = new (std::nothrow) vsfeel_bm3d_batch();
+    if (!b) return error(VSFEEL_E_MEMORY, "out of host memory");
+    b->device = device;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(device);
+    int rc = VSFEEL_OK;
+    try {
+        std::map<ClassKey, int> index;
+        for (int i = 0; i < nclips; ++i) {
+            const vsfeel_bm3d_batch_clip& d = clips[i];
+            Clip c;
+            c.desc = d;
+            if (d.args.has_ref)
+                throw Fail{VSFEEL_E_UNSUPPORTED, "clip " + std::to_string(i) +
+                                                     ": the final (Wiener) pass with \"ref\" is not "
+                                                     "supported by this build"};
+            vsfeel_bm3d_video_info vi{d.width, d.height, d.num_frames, VSFEEL_CF_GRAY,
+                                      VSFEEL_ST_FLOAT, 32, 0, 0};
+            if (const int prc = parse_to_info(&d.args, &vi, &c.info); prc != VSFEEL_OK) {
+                std::string msg = vsfeel_bm3d_last_error();
+                if (msg.rfind("BM3D: ", 0) == 0) msg = msg.substr(6);
+                throw Fail{prc, "clip " + std::to_string(i) + ": " + msg};
+            }
+            if (!d.src || !d.dst) throw Fail{VSFEEL_E_ARG, "clip " + std::to_string(i) + ": null buffer"};
+            if (d.src_row_stride < d.width || d.dst_row_stride < d.width ||
+                d.src_row_stride > INT32_MAX || d.dst_row_stride > INT32_MAX)
+                throw Fail{VSFEEL_E_ARG, "clip " + std::to_string(i) + ": row stride smaller than the width"};
+            if (d.src_frame_stride < d.src_row_stride * d.height ||
+                d.dst_frame_stride < d.dst_row_stride * d.height)
+                throw Fail{VSFEEL_E_ARG, "clip " + std::to_string(i) + ": frame stride smaller than a plane"};
+            c.acc_pitch = (d.width + 31) & ~31;
+            c.plane = (size_t)d.height * c.acc_pitch;
+            b->clips.push_back(c);
+            const ClassKey key{c.info.radius, c.info.block_step, c.info.bm_range, c.info.ps_num,
+                               c.info.ps_range};
+            auto it = index.find(key);
+            if (it == index.end()) {
+                it = index.emplace(key, (int)b->classes.size()).first;
+                b->classes.emplace_back();
+                b->classes.back().key = key;
+            }
+            b->classes[it->second].clips.push_back(i);
+        }
+        check(cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, device), "attribute");
+        b->status.alloc(1);
+        check(cudaMemset(b->status.p, 0, sizeof(int)), "cudaMemset");
+        check(cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming), "cudaEventCreate");
+        const int forced = ((flags >> 4) & 15) - 1;
+        for (Class& cls : b->classes)
+            build_class(b, cls, (flags & VSFEEL_BATCH_AUTOTUNE) != 0, forced);
+    } catch (const Fail& f) {
+        rc = error(f.code, f.msg);
+    } catch (const std::bad_alloc&) {
+        rc = error(VSFEEL_E_MEMORY, "out of host memory");
+    }
+    if (rc != VSFEEL_OK) {
+        delete b;
+        if (prev >= 0) cudaSetDevice(prev);
+        return rc;
+    }
+    if (prev >= 0) cudaSetDevice(prev);
+    *out = b;
+    return VSFEEL_OK;
+}
+
+int vsfeel_bm3d_batch_run(vsfeel_bm3d_batch* b, void* stream) {
+    if (!b) return error(VSFEEL_E_ARG, "null batch");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(b->device);
+    int rc = VSFEEL_OK;
+    try {
+        cudaStream_t st = (cudaStream_t)stream;
+        check(cudaEventRecord(b->start, st), "cudaEventRecord");
+        for (Class& c : b->classes) {
+            check(cudaStreamWaitEvent(c.stream, b->start, 0), "cudaStreamWaitEvent");
+            check(cudaGraphLaunch(c.exec, c.stream), "cudaGraphLaunch");
+            check(cudaEventRecord(c.done, c.stream), "cudaEventRecord");
+            check(cudaStreamWaitEvent(st, c.done, 0), "cudaStreamWaitEvent");
+        }
+    } catch (const Fail& f) {
+        rc = error(f.code, f.msg);
+    }
+    if (prev >= 0) cudaSetDevice(prev);
+    return rc;
+}
+
+int vsfeel_bm3d_batch_finish(vsfeel_bm3d_batch* b) {
+    if (!b) return error(VSFEEL_E_ARG, "null batch");
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(b->device);
+    int rc = VSFEEL_OK;
+    for (Class& c : b->classes)
+        if (rc == VSFEEL_OK) rc = wait_stream(c.stream);
+    if (rc == VSFEEL_OK) {
+        int word = 0;
+        cudaError_t e = cudaMemcpy(&word, b->status.p, sizeof(int), cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) {
+            rc = error(VSFEEL_E_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+        } else if (word != 0) {
+            cudaMemset(b->status.p, 0, sizeof(int));
+            rc = error(VSFEEL_E_CUDA, "internal error: a search window left the staged region");
+        }
+    }
+    if (prev >= 0) cudaSetDevice(prev);
+    return rc;
+}
+
+int vsfeel_bm3d_batch_classes(const vsfeel_bm3d_batch* b, int* nclasses, int64_t* device_bytes) {
+    if (!b || !nclasses || !device_bytes) return error(VSFEEL_E_ARG, "null argument");
+    *nclasses = (int)b->classes.size();
+    *device_bytes = b->device_bytes;
+    return VSFEEL_OK;
+}
+
+int vsfeel_bm3d_batch_class(const vsfeel_bm3d_batch* b, int index,
+                            vsfeel_bm3d_batch_class_info* info) {
+    if (!b || !info) return error(VSFEEL_E_ARG, "null argument");
+    if (index < 0 || index >= (int)b->classes.size()) return error(VSFEEL_E_ARG, "class index out of range");
+    const Class& c = b->classes[index];
+    std::memset(info, 0, sizeof(*info));
+    info->radius = std::get<0>(c.key);
+    info->block_step = std::get<1>(c.key);
+    info->bm_range = std::get<2>(c.key);
+    info->ps_num = std::get<3>(c.key);
+    info->ps_range = std::get<4>(c.key);
+    info->clips = (int)c.clips.size();
+    info->stacks = (int)c.jobs.size();
+    info->tiles = c.tiles;
+    info->tile_shape = c.tile_shape;
+    for (int s = 0; s < kTileShapes && s < VSFEEL_TILE_SHAPES; ++s) info->tuned_ms[s] = c.tuned_ms[s];
+    return VSFEEL_OK;
+}
+
+void vsfeel_bm3d_batch_free(vsfeel_bm3d_batch* b) {
+    if (!b) return;
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(b->device);
+    delete b;
+    if (prev >= 0) cudaSetDevice(prev);
+}
+
+}  // extern "C"

@@ -48,6 +48,14 @@ struct NormalizeJob {
     int den_pitch;
 };
 
+// Many normalisations in one launch: output j covers the items
+// tile_first[j] .. tile_first[j+1]-1, one 32x8-pixel tile each.
+struct NormalizeBatch {
+    const NormalizeJob* jobs;
+    const int* tile_first;
+    int njobs;
+};
+
 // Adjoint of the frozen-match operator over a whole clip: one launch covers
 // every block of every stack. The saved state is what the forward pass
 // recorded per stack (match table and keep bits) plus the per-output
@@ -68,14 +76,48 @@ struct AdjointJob {
     int width, height;           // match positions are clamped to the frame
 };
 
+// Tiled matcher (bm3d_match.cu): tile shapes in blocks, and what a tile
+// does after matching.
+enum TileShape { kTile8x4 = 0, kTile16x2, kTile4x8, kTile8x2, kTile4x4, kTileShapes };
+enum TileMode { kTableOnly = 0, kFused = 1, kFusedSave = 2 };
+
+// The persistent form's work queue: tiles of jobs[0..njobs), job j owning
+// items tile_first[j] .. tile_first[j+1]-1; counter is zeroed before a launch.
+struct BatchWork {
+    const StackJob* jobs;
+    const int* tile_first;
+    int njobs;
+    int* counter;
+};
+
 // Host-side launchers (defined beside the kernels). Each returns the launch
 // status and enqueues on `stream`.
 cudaError_t launch_match(const StackJob& job, cudaStream_t stream);
-cudaError_t launch_match_sliding(const StackJob& job, cudaStream_t stream);
-bool match_sliding_fits(const StackJob& job);
 cudaError_t launch_filter(const StackJob& job, cudaStream_t stream);
+const char* tile_shape_name(TileShape shape);
+bool tile_shape_fits(const StackJob& job, TileShape shape, TileMode mode);
+int default_tile_shape(const StackJob& job, TileMode mode);  // -1: none fits
+size_t tile_smem_bytes(const StackJob& job, TileShape shape, TileMode mode);
+int tile_count(const StackJob& job, TileShape shape);
+cudaError_t launch_match_tiles(const StackJob& job, TileShape shape, TileMode mode,
+                               cudaStream_t stream);
+cudaError_t launch_batch_tiles(const BatchWork& work, TileShape shape, TileMode mode, size_t smem,
+                               int grid, cudaStream_t stream);  // mode: kTableOnly or kFused
+
+// Many stacks' filters in one launch: job j covers the items
+// group_first[j] .. group_first[j+1]-1, 16 groups (blocks) each, with its
+// matches in its own match table.
+struct FilterBatch {
+    const StackJob* jobs;
+    const int* group_first;
+    int njobs;
+};
+cudaError_t launch_filter_batch(const FilterBatch& work, int total_items, cudaStream_t stream);
+inline int filter_items(int nblocks) { return (nblocks + 15) / 16; }
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream);
 cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream);
+cudaError_t launch_normalize_batch(const NormalizeBatch& work, int total_tiles, cudaStream_t stream);
+inline int normalize_tiles(int width, int height) { return ((width + 31) / 32) * ((height + 7) / 8); }
 
 __host__ __device__ inline int block_count(int extent, int step) {
     return (extent - 9 + 2 * step) / step;  // positions x0 = b*step < extent - 8 + step

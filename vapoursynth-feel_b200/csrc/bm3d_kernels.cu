@@ -16,6 +16,7 @@
 // ordered by (SSD, scan index), so the merged list is the 8 smallest keys,
 // exactly as in the reference.
 #include "bm3d_device.cuh"
+#include "bm3d_filter.cuh"
 
 namespace vsfeel {
 
@@ -260,139 +261,21 @@ __global__ void __launch_bounds__(128) bm3d_match_kernel(const StackJob job) {
     }
 }
 
-// ---------------------------------------------------------------------------
-// Filtering. Lane sub of a group holds column sub of the 8 matched patches:
-// d[k*8 + j] = patch k, row j. The 3D transform runs in the reference's axis
-// order (rows of each column, columns of each row, then along the group; the
-// inverse in the same order), with 8x8 transposes through shared memory.
-
-namespace {
-
-constexpr int kRowStride = 9;                 // floats per transposed row
-constexpr int kTileStride = 8 * kRowStride;   // one 8x8 tile
-constexpr int kGroupStride = 8 * kTileStride + 8;  // one group's 8 tiles (+8: bank skew)
-constexpr int kGroupsPerCta = 16;
-
-// new d_l[k*8 + i] = old d_i[k*8 + l] within each group
-__device__ __forceinline__ void transpose_group(float d[64], float* buf, int sub) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) buf[k * kTileStride + i * kRowStride + sub] = d[k * 8 + i];
-    __syncwarp();
-#pragma unroll
-    for (int k = 0; k < 8; ++k)
-#pragma unroll
-        for (int i = 0; i < 8; ++i) d[k * 8 + i] = buf[k * kTileStride + sub * kRowStride + i];
-    __syncwarp();
-}
-
-__device__ __forceinline__ void transform_rows(float d[64], bool inverse) {
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        if (inverse)
-            dct8_inv(&d[k * 8]);
-        else
-            dct8_fwd(&d[k * 8]);
-    }
-}
-
-__device__ __forceinline__ void transform_group_axis(float d[64], bool inverse) {
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-        float v[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = d[k * 8 + i];
-        if (inverse)
-            dct8_inv(v);
-        else
-            dct8_fwd(v);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) d[k * 8 + i] = v[k];
-    }
-}
-
-}  // namespace
-
-// kSaveMask: also record the keep bits of every coefficient, lane `sub`
-// writing word mask_out[block * 8 + sub] (bit 8 * group_freq + vertical_freq
-// of horizontal frequency `sub`), for the adjoint.
+// The standalone filter: 16 groups of 8 lanes per CTA, matches read from
+// the stack's match table.
 template <bool kSaveMask>
 __global__ void __launch_bounds__(128) bm3d_filter_kernel(const StackJob job) {
-    __shared__ float smem[kGroupsPerCta / 4 * 4 * kGroupStride];
-    const int lane = threadIdx.x & 31;
-    const int sub = lane & 7;
-    const int group_in_cta = threadIdx.x >> 3;
-    float* buf = smem + group_in_cta * kGroupStride;
+    __shared__ float smem[kFilterGroupsPerCta * kGroupStride];
+    const int sub = threadIdx.x & 7;
+    float* buf = smem + (threadIdx.x >> 3) * kGroupStride;
     const int nblocks = job.nbx * job.nby;
     const int gblock = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 3);
     const bool valid = gblock < nblocks;
     const int b = valid ? gblock : nblocks - 1;
-
     const uint4 m0 = reinterpret_cast<const uint4*>(job.match_xy + (size_t)b * 8)[0];
     const uint4 m1 = reinterpret_cast<const uint4*>(job.match_xy + (size_t)b * 8)[1];
     const uint32_t mxy[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
-    const uint32_t zp = job.match_z[b];
-    const int pitch = job.pitch;
-
-    float d[64];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int z = (int)((zp >> (4 * k)) & 15u);
-        const float* __restrict__ f = job.slice_frame[z];
-        const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
-        const float* p = f + (size_t)my * pitch + mx + sub;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) d[k * 8 + j] = __ldg(p + (size_t)j * pitch);
-    }
-
-    transform_rows(d, false);
-    transpose_group(d, buf, sub);
-    transform_rows(d, false);
-    transpose_group(d, buf, sub);
-    transform_group_axis(d, false);
-
-    const float thr = job.thr;
-    int kept = 0;
-    uint64_t bits = 0;
-#pragma unroll
-    for (int i = 0; i < 64; ++i) {
-        const float t = (i == 0 && sub == 0) ? 0.0f : thr;
-        const bool keep = fabsf(d[i]) >= t;
-        kept += keep ? 1 : 0;
-        if (kSaveMask) bits |= keep ? (uint64_t(1) << i) : uint64_t(0);
-        d[i] = keep ? __fmul_rn(d[i], 1.0f / 4096.0f) : 0.0f;
-    }
-    if (kSaveMask && valid) job.mask_out[(size_t)b * 8 + sub] = bits;
-    kept += __shfl_xor_sync(kFull, kept, 1);
-    kept += __shfl_xor_sync(kFull, kept, 2);
-    kept += __shfl_xor_sync(kFull, kept, 4);
-    const float w = __fdiv_rn(1.0f, (float)kept);
-
-    transform_rows(d, true);
-    transpose_group(d, buf, sub);
-    transform_rows(d, true);
-    transpose_group(d, buf, sub);
-    transform_group_axis(d, true);
-
-    if (!valid) return;
-    const float E = job.extractor;
-    const float wv = __fsub_rn(__fadd_rn(w, E), E);
-    const int dpitch = job.dst_pitch;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int z = (int)((zp >> (4 * k)) & 15u);
-        float* num = job.slice_dst[z];
-        if (num == nullptr) continue;
-        const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
-        float* pn = num + (size_t)my * dpitch + mx + sub;
-        float* pd = pn + job.dst_plane;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            atomicAdd(pn + (size_t)j * dpitch, __fsub_rn(__fmaf_rn(w, d[k * 8 + j], E), E));
-            atomicAdd(pd + (size_t)j * dpitch, wv);
-        }
-    }
+    filter_group<kSaveMask>(job, b, valid, mxy, job.match_z[b], sub, buf);
 }
 
 // ---------------------------------------------------------------------------
@@ -410,6 +293,57 @@ __global__ void __launch_bounds__(256) bm3d_normalize_kernel(const NormalizeJob 
     if (job.den_out) job.den_out[(size_t)y * job.den_pitch + x] = (float)acw;
 }
 
+// Batched form: the filter of 16 blocks of one stack per CTA.
+__global__ void __launch_bounds__(128) bm3d_filter_batch_kernel(const FilterBatch work) {
+    __shared__ float smem[kFilterGroupsPerCta * kGroupStride];
+    const int item = blockIdx.x;
+    int lo = 0, hi = work.njobs - 1;
+    while (lo < hi) {  // last job whose first item is <= item
+        const int mid = (lo + hi + 1) >> 1;
+        if (work.group_first[mid] <= item)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const StackJob& job = work.jobs[lo];
+    const int sub = threadIdx.x & 7;
+    float* buf = smem + (threadIdx.x >> 3) * kGroupStride;
+    const int nblocks = job.nbx * job.nby;
+    const int gblock = (item - work.group_first[lo]) * 16 + (threadIdx.x >> 3);
+    const bool valid = gblock < nblocks;
+    const int b = valid ? gblock : nblocks - 1;
+    const uint4 m0 = reinterpret_cast<const uint4*>(job.match_xy + (size_t)b * 8)[0];
+    const uint4 m1 = reinterpret_cast<const uint4*>(job.match_xy + (size_t)b * 8)[1];
+    const uint32_t mxy[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
+    filter_group<false>(job, b, valid, mxy, job.match_z[b], sub, buf);
+}
+
+// Batched form: one CTA per 32x8 tile of one output frame.
+__global__ void __launch_bounds__(256) bm3d_normalize_batch_kernel(const NormalizeBatch work) {
+    const int item = blockIdx.x;
+    int lo = 0, hi = work.njobs - 1;
+    while (lo < hi) {  // last job whose first tile is <= item
+        const int mid = (lo + hi + 1) >> 1;
+        if (work.tile_first[mid] <= item)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    const NormalizeJob& job = work.jobs[lo];
+    const int t = item - work.tile_first[lo];
+    const int tiles_x = (job.width + 31) / 32;
+    const int x = (t % tiles_x) * 32 + (threadIdx.x & 31);
+    const int y = (t / tiles_x) * 8 + (threadIdx.x >> 5);
+    if (x >= job.width || y >= job.height) return;
+    const size_t o = (size_t)y * job.src_pitch + x;
+    double acc = 0.0, acw = 0.0;
+    for (int i = 0; i < job.tw; ++i) {
+        acc += (double)job.num[i][o];
+        acw += (double)job.num[i][o + job.den_offset];
+    }
+    job.out[(size_t)y * job.out_pitch + x] = (float)(acc / acw);
+}
+
 // ---------------------------------------------------------------------------
 // Adjoint of the frozen-match operator (no counterpart in the reference).
 //
@@ -425,7 +359,7 @@ __global__ void __launch_bounds__(256) bm3d_normalize_kernel(const NormalizeJob 
 // scatter-add into the input gradient of the same patches. The extractor's
 // rounding of the forward scatter is taken as the identity.
 __global__ void __launch_bounds__(128) bm3d_adjoint_kernel(const AdjointJob job) {
-    __shared__ float smem[kGroupsPerCta / 4 * 4 * kGroupStride];
+    __shared__ float smem[kFilterGroupsPerCta * kGroupStride];
     const int lane = threadIdx.x & 31;
     const int sub = lane & 7;
     const int group_in_cta = threadIdx.x >> 3;
@@ -510,7 +444,8 @@ int block_grid(const StackJob& job) { return (job.nbx * job.nby * 8 + kThreads -
 
 cudaError_t launch_match(const StackJob& job, cudaStream_t stream) {
     if (job.radius < 3) {
-        if (match_sliding_fits(job)) return launch_match_sliding(job, stream);
+        const int shape = default_tile_shape(job, kTableOnly);
+        if (shape >= 0) return launch_match_tiles(job, TileShape(shape), kTableOnly, stream);
         bm3d_match_kernel<true><<<block_grid(job), kThreads, 0, stream>>>(job);
     } else {
         bm3d_match_kernel<false><<<block_grid(job), kThreads, 0, stream>>>(job);
@@ -523,6 +458,19 @@ cudaError_t launch_filter(const StackJob& job, cudaStream_t stream) {
         bm3d_filter_kernel<true><<<block_grid(job), kThreads, 0, stream>>>(job);
     else
         bm3d_filter_kernel<false><<<block_grid(job), kThreads, 0, stream>>>(job);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_filter_batch(const FilterBatch& work, int total_items, cudaStream_t stream) {
+    if (total_items <= 0) return cudaSuccess;
+    bm3d_filter_batch_kernel<<<total_items, kThreads, 0, stream>>>(work);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normalize_batch(const NormalizeBatch& work, int total_tiles,
+                                   cudaStream_t stream) {
+    if (total_tiles <= 0) return cudaSuccess;
+    bm3d_normalize_batch_kernel<<<total_tiles, 256, 0, stream>>>(work);
     return cudaGetLastError();
 }
 

@@ -1,581 +1,68 @@
-// Block matching for radius < 3: the reference's sliding column scan
-// (src/bm3d.comp:479-538 spatial, 540-637 temporal), restructured for sm_100a.
-//
-// A CTA owns a tile of 8x4 reference blocks, 8 lanes per block; a warp holds
-// four blocks of one block row, two block columns apart. For each search
-// phase (the spatial window in frame m, then one temporal step per frame) the
-// CTA stages the frame region that every window of the tile can reach
-// (tile +- bm_range + t*ps_range) in shared memory once, column-major.
-//
-// Scan. Within a block, lane s takes a chunk of K consecutive candidate rows
-// of a window and sweeps the window's columns left to right. One step loads
-// the K+7 source values of column X (consecutive words), updates the K
-// column sums
-//     V(X) = SSD(source column X, block column min(X - left, 7))
-// and advances, per row, the reduction tree of the reference in incremental
-// form: P(j) = V(j) + V(j+1), Q(j) = P(j) + P(j+2), E(j) = Q(j) + Q(j+4) --
-// the same additions on the same operands as
-// ((c0+c1)+(c2+c3))+((c4+c5)+(c6+c7)), so every candidate error carries the
-// reference's bits. Every error is stored to the block's error table in
-// shared memory; the lane also keeps each row's two smallest errors.
-//
-// Selection. The reference keeps per-lane sorted top-8 lists and merges them
-// by (error, scan index); the result is the 8 smallest (error, index) keys.
-// Here the block's 8 lanes bound the 8th smallest error by the 8th smallest
-// of the window rows' two smallest errors, collect the few candidates at or
-// below the bound from the table, and place each by counting the collected
-// keys below it. The scan itself carries no branches or votes.
+// Host side of the tiled matcher: tile shapes, shared-memory fitting and
+// the dispatch to the per-shape instantiations (bm3d_match_<shape>.cu; the
+// kernels themselves are in bm3d_match.cuh).
 #include "bm3d_device.cuh"
 
 #include <algorithm>
 
 namespace vsfeel {
 
+#define VSFEEL_TILE_DECL(TX, TY)                                                              \
+    size_t tile_plan_bytes_##TX##x##TY(const StackJob& job, TileMode mode);                   \
+    cudaError_t launch_tiles_##TX##x##TY(const StackJob& job, TileMode mode, cudaStream_t s); \
+    cudaError_t launch_batch_##TX##x##TY(const BatchWork& work, TileMode mode, size_t smem,   \
+                                         int grid, cudaStream_t s);
+VSFEEL_TILE_DECL(8, 4)
+VSFEEL_TILE_DECL(16, 2)
+VSFEEL_TILE_DECL(4, 8)
+VSFEEL_TILE_DECL(8, 2)
+VSFEEL_TILE_DECL(4, 4)
+#undef VSFEEL_TILE_DECL
+
 namespace {
 
-constexpr unsigned kFull = 0xffffffffu;
-constexpr int kTileBX = 8, kTileBY = 4;
-constexpr int kGroups = kTileBX * kTileBY;
-constexpr int kMatchThreads = kGroups * 8;  // 256
-constexpr int kMinK = 2, kMaxK = 5;
-constexpr int kCollect = 64;                // candidates a block collects per pass
-constexpr uint64_t kKeyMax = (uint64_t(0x7f7fffffu) << 32) | 0x7fffffffu;  // (FLT_MAX, INT_MAX)
-
-__device__ __forceinline__ uint64_t make_key(float err, int seq) {
-    return (uint64_t(__float_as_uint(err)) << 32) | uint32_t(seq);
-}
-
-__device__ __forceinline__ float key_err(uint64_t k) { return __uint_as_float(uint32_t(k >> 32)); }
-
-__device__ __forceinline__ int warp_max(int v) {
-#pragma unroll
-    for (int off = 1; off < 32; off <<= 1) v = max(v, __shfl_xor_sync(kFull, v, off));
-    return v;
-}
-
-// A search window: candidate columns left..left+rw-1, rows top..top+h-1,
-// scan indices seq_base + (cy-top)*rw + (cx-left); its errors sit in the
-// block's table at eoff + (cx-left)*h + (cy-top).
-struct Window {
-    int left, top, rw, h, seq_base, eoff;
+struct ShapeInfo {
+    int tx, ty;
 };
+constexpr ShapeInfo kShapes[kTileShapes] = {{8, 4}, {16, 2}, {4, 8}, {8, 2}, {4, 4}};
+constexpr size_t kSmemBudget = 220 * 1024;
 
-__device__ __forceinline__ Window make_window(int cx, int cy, int range, int width, int height,
-                                              int seq_base, int eoff) {
-    Window w;
-    w.left = max(cx - range, 0);
-    const int right = min(cx + range, width - 8);
-    w.top = max(cy - range, 0);
-    const int bottom = min(cy + range, height - 8);
-    w.rw = right - w.left + 1;
-    w.h = bottom - w.top + 1;
-    w.seq_base = seq_base;
-    w.eoff = eoff;
-    return w;
-}
-
-// The staged region, column-major with column stride cs (odd), so the K+7
-// source rows a lane needs at one column are consecutive words.
-struct Region {
-    const float* smem;
-    int rx0, ry0, cs;
-    int rx1, ry1;  // last staged column and row
-};
-
-// SSD of one column of the block (bc) against w[q..q+7].
-template <int K>
-__device__ __forceinline__ float column_ssd_at(const float bc[8], const float w[K + 7], int q) {
-    float ev = 0.0f, od = 0.0f;
-#pragma unroll
-    for (int i = 0; i < 8; i += 2) {
-        const float d0 = __fsub_rn(bc[i], w[q + i]);
-        ev = __fmaf_rn(d0, d0, ev);
-        const float d1 = __fsub_rn(bc[i + 1], w[q + i + 1]);
-        od = __fmaf_rn(d1, d1, od);
+size_t plan_bytes(const StackJob& job, TileShape shape, TileMode mode) {
+    switch (shape) {
+        case kTile8x4: return tile_plan_bytes_8x4(job, mode);
+        case kTile16x2: return tile_plan_bytes_16x2(job, mode);
+        case kTile4x8: return tile_plan_bytes_4x8(job, mode);
+        case kTile8x2: return tile_plan_bytes_8x2(job, mode);
+        default: return tile_plan_bytes_4x4(job, mode);
     }
-    return __fadd_rn(ev, od);
-}
-
-// One lane's chunk: rows r0..r0+nrows-1 of window `win` (nrows may be 0),
-// `jcount` column steps (warp-uniform; steps past the window's width are
-// padding). cur_s: the block's 64 values in shared memory, column-major; c7:
-// block column 7 in registers. Errors go to table E; each row's two smallest
-// errors are merged into lb, this lane's 8 smallest such values (ascending).
-template <int K>
-__device__ __forceinline__ void scan_chunk(const Region& reg, const float* cur_s, const float c7[8],
-                                           const Window& win, int r0, int nrows, int jcount,
-                                           float* E, float lb[8]) {
-    float vp[K], pr[K][2], qr[K][4];
-    float m1[K], m2[K];
-#pragma unroll
-    for (int q = 0; q < K; ++q) m1[q] = m2[q] = kFltMax;
-    const int xmax = win.left + win.rw + 6;
-    // rows past the window exist in each staged column (padding) and only
-    // feed masked rows
-    const float* sbase = reg.smem + (r0 - reg.ry0) - reg.rx0 * reg.cs;
-    const int cs = reg.cs;
-    float* ecol = E + win.eoff + (r0 - win.top);
-
-    auto load_col = [&](int X, float w[K + 7]) {
-        const float* col = sbase + X * cs;
-#pragma unroll
-        for (int k = 0; k < K + 7; ++k) w[k] = col[k];
-    };
-    auto emit = [&](const float e[K], int d) {
-        if (d < win.rw) {
-            float* out = ecol + d * win.h;
-#pragma unroll
-            for (int q = 0; q < K; ++q) {
-                if (q < nrows) {
-                    out[q] = e[q];
-                    m2[q] = fminf(m2[q], fmaxf(m1[q], e[q]));
-                    m1[q] = fminf(m1[q], e[q]);
-                }
-            }
-        }
-    };
-
-    // warm-up: block columns 0..7, steps j = 0..7 (candidate column 0 at j = 7)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        float bc[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) bc[i] = (j == 7) ? c7[i] : cur_s[j * 8 + i];
-        float w[K + 7];
-        load_col(min(win.left + j, xmax), w);
-        float e[K];
-#pragma unroll
-        for (int q = 0; q < K; ++q) {
-            const float v = column_ssd_at<K>(bc, w, q);
-            e[q] = 0.0f;
-            if (j >= 1) {
-                const float np = __fadd_rn(vp[q], v);  // P(j-1)
-                if (j >= 3) {
-                    const float nq = __fadd_rn(pr[q][(j + 1) & 1], np);  // Q(j-3)
-                    if (j == 7) e[q] = __fadd_rn(qr[q][0], nq);          // E(0)
-                    qr[q][(j + 1) & 3] = nq;
-                }
-                pr[q][(j + 1) & 1] = np;
-            }
-            vp[q] = v;
-        }
-        if (j == 7) emit(e, 0);
-    }
-    // steady state: block column 7, steps j = 8 .. jcount-1, four per
-    // iteration so that the ring positions are static
-    for (int j0 = 8; j0 < jcount; j0 += 4) {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int j = j0 + u;
-            float w[K + 7];
-            load_col(min(win.left + j, xmax), w);
-            float e[K];
-#pragma unroll
-            for (int q = 0; q < K; ++q) {
-                const float v = column_ssd_at<K>(c7, w, q);
-                const float np = __fadd_rn(vp[q], v);
-                const float nq = __fadd_rn(pr[q][(u + 1) & 1], np);
-                e[q] = __fadd_rn(qr[q][(u + 1) & 3], nq);
-                pr[q][(u + 1) & 1] = np;
-                qr[q][(u + 1) & 3] = nq;
-                vp[q] = v;
-            }
-            if (j < jcount) emit(e, j - 7);
-        }
-    }
-    // merge the rows' two smallest into the lane's 8 smallest
-#pragma unroll
-    for (int q = 0; q < 2 * K; ++q) {
-        float c = q < K ? m1[q] : m2[q - K];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float lo = fminf(lb[i], c);
-            c = fmaxf(lb[i], c);
-            lb[i] = lo;
-        }
-    }
-}
-
-__device__ __forceinline__ int rows_per_lane(int total_rows) {
-    return min(kMaxK, max(kMinK, (total_rows + 7) / 8));
-}
-
-// A block's global match list, spatial predictors, the phase's top-8 and the
-// collection buffer (src/bm3d.comp:469-470, 541-545, 622-633).
-struct GroupState {
-    float ge[8];
-    uint32_t gxy[8];
-    int gz[8];
-    uint32_t sxy[8];
-    uint32_t pxy[8];
-    uint64_t top[8];
-    uint64_t buf[kCollect];
-    int count;
-};
-
-// The 8 smallest (error, scan index) keys of the windows' error table into
-// gs->top (padded with (FLT_MAX, INT_MAX) when fewer exist; errors >= FLT_MAX
-// never count, as in the reference). lb: this lane's 8 smallest per-row
-// minima (ascending). All 8 lanes of the group take part.
-__device__ void select_top8(const float* E, const Window* wins, int nwin, float lb[8],
-                            GroupState* gs, unsigned gmask) {
-    const int sub = threadIdx.x & 7;
-    // bound: the 8th smallest of the rows' two smallest errors -- at least 8
-    // candidates lie at or below it
-    float bound = kFltMax;
-#pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        float best = lb[0];
-        int src = sub;
-#pragma unroll
-        for (int off = 1; off < 8; off <<= 1) {
-            const float o = __shfl_xor_sync(gmask, best, off);
-            const int os = __shfl_xor_sync(gmask, src, off);
-            const bool take = o < best || (o == best && os < src);
-            best = take ? o : best;
-            src = take ? os : src;
-        }
-        bound = best;
-        if (sub == src) {
-#pragma unroll
-            for (int i = 0; i < 7; ++i) lb[i] = lb[i + 1];
-            lb[7] = kFltMax;
-        }
-    }
-    uint64_t tkey = (uint64_t(__float_as_uint(bound)) << 32) | 0xffffffffu;
-    int n;
-    for (;;) {
-        if (sub == 0) gs->count = 0;
-        __syncwarp(gmask);
-        const float terr = key_err(tkey);
-        const uint32_t tseq = uint32_t(tkey);
-        // a window's table is rw*h contiguous words from a 4-aligned offset:
-        // sweep it four entries per load, 32 per group step
-        for (int wi = 0; wi < nwin; ++wi) {
-            const Window w = wins[wi];
-            const int n_w = w.rw * w.h;
-            const float4* tab = reinterpret_cast<const float4*>(E + w.eoff);
-            for (int v = sub; 4 * v < n_w; v += 8) {
-                const float4 q = tab[v];
-                const float ev[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int f = 4 * v + u;
-                    if (f < n_w && ev[u] <= terr && ev[u] < kFltMax) {
-                        const int d = f / w.h;
-                        const int row = f - d * w.h;
-                        const uint32_t seq = uint32_t(w.seq_base + row * w.rw + d);
-                        if (ev[u] < terr || seq <= tseq) {
-                            const int pos = atomicAdd(&gs->count, 1);
-                            if (pos < kCollect) gs->buf[pos] = make_key(ev[u], int(seq));
-                        }
-                    }
-                }
-            }
-        }
-        __syncwarp(gmask);
-        n = gs->count;
-        if (n <= kCollect) break;
-        // more than kCollect at or below the bound: tighten it to the 8th
-        // smallest key among the collected ones and collect again
-        uint64_t t8 = kKeyMax;
-        for (int j = sub; j < kCollect; j += 8) {
-            const uint64_t kj = gs->buf[j];
-            int rank = 0;
-            for (int i = 0; i < kCollect; ++i) rank += gs->buf[i] < kj ? 1 : 0;
-            if (rank == 7) t8 = kj;
-        }
-#pragma unroll
-        for (int off = 1; off < 8; off <<= 1) {
-            const uint64_t o = __shfl_xor_sync(gmask, t8, off);
-            t8 = o < t8 ? o : t8;
-        }
-        tkey = t8;
-        __syncwarp(gmask);
-    }
-    gs->top[sub] = kKeyMax;
-    __syncwarp(gmask);
-    for (int j = sub; j < n; j += 8) {
-        const uint64_t kj = gs->buf[j];
-        int rank = 0;
-        for (int i = 0; i < n; ++i) rank += gs->buf[i] < kj ? 1 : 0;
-        if (rank < 8) gs->top[rank] = kj;
-    }
-    __syncwarp(gmask);
-}
-
-// Scans windows[0..nwin) of this lane's block into its error table, then
-// selects the top-8 into gs->top. Rows are split into chunks of K
-// (warp-uniform); chunk c of the block goes to lane c % 8 in round c / 8.
-__device__ void search_windows(const Region& reg, const float* cur_s, const float c7[8],
-                               const Window* wins, int nwin, float* E, GroupState* gs,
-                               unsigned gmask, int* status) {
-    const int sub = threadIdx.x & 7;
-    int total_rows = 0;
-    for (int i = 0; i < nwin; ++i) total_rows += wins[i].h;
-    const int K = warp_max(rows_per_lane(total_rows));
-    int ntasks = 0;
-    for (int i = 0; i < nwin; ++i) ntasks += (wins[i].h + K - 1) / K;
-    const int rounds = warp_max((ntasks + 7) / 8);
-    float lb[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) lb[i] = kFltMax;
-    for (int round = 0; round < rounds; ++round) {
-        const int task = round * 8 + sub;
-        const bool has = task < ntasks;
-        int wi = 0, c = has ? task : 0;
-        while (wi < nwin - 1 && c >= (wins[wi].h + K - 1) / K) {
-            c -= (wins[wi].h + K - 1) / K;
-            ++wi;
-        }
-        Window win = wins[wi];
-        int r0 = win.top + c * K;
-        int nrows = has ? min(K, win.h - c * K) : 0;
-        // every window lies inside the staged region by construction (the
-        // host routes configurations that could place one outside to the
-        // direct-read kernel); should one not, scan nothing here and report
-        if (win.left < reg.rx0 || win.left + win.rw + 6 > reg.rx1 || win.top < reg.ry0 ||
-            win.top + win.h + 6 > reg.ry1) {
-            if (has) atomicOr(status, 1);
-            win = Window{reg.rx0, reg.ry0, 1, 1, 0, 0};
-            r0 = reg.ry0;
-            nrows = 0;
-        }
-        const int jcount = warp_max(has ? win.rw + 7 : 8);
-        switch (K) {
-            case 2: scan_chunk<2>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
-            case 3: scan_chunk<3>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
-            case 4: scan_chunk<4>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
-            default: scan_chunk<5>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
-        }
-    }
-    __syncwarp(gmask);
-    select_top8(E, wins, nwin, lb, gs, gmask);
-}
-
-// global list insertion of a temporal match (src/bm3d.comp:304-322)
-__device__ __forceinline__ void ginsert(float ge[8], uint32_t gxy[8], int gz[8], float err,
-                                        uint32_t cxy, int cz) {
-    if (err < ge[7]) {
-        int pos = 7;
-        while (pos > 0 && err < ge[pos - 1]) {
-            ge[pos] = ge[pos - 1];
-            gxy[pos] = gxy[pos - 1];
-            gz[pos] = gz[pos - 1];
-            --pos;
-        }
-        ge[pos] = err;
-        gxy[pos] = cxy;
-        gz[pos] = cz;
-    }
-}
-
-// Position of a key. Sentinels decode to (0, 0) as in the reference.
-__device__ __forceinline__ uint32_t key_xy(uint64_t key, const Window* wins, int area) {
-    if (key == kKeyMax) return 0u;
-    const int seq = int(uint32_t(key));
-    const int wi = area > 0 ? seq / area : 0;
-    const Window w = wins[wi];
-    const int rem = seq - w.seq_base;
-    const int dy = rem / w.rw;
-    const int dx = rem - dy * w.rw;
-    return uint32_t(w.left + dx) | (uint32_t(w.top + dy) << 16);
-}
-
-// Stages frame rows [ry0, ry1] x columns [rx0, rx1] into smem, column-major
-// with column stride cs (odd, so the transposing stores of a warp hit
-// distinct banks). Global reads are coalesced along rows.
-__device__ void stage_region(float* smem, const float* __restrict__ frame, int pitch, int rx0,
-                             int ry0, int rx1, int ry1, int cs) {
-    const int w = rx1 - rx0 + 1;
-    const int h = ry1 - ry0 + 1;
-    const int lane = threadIdx.x & 31;
-    for (int yy = threadIdx.x >> 5; yy < h; yy += blockDim.x >> 5) {
-        const float* __restrict__ row = frame + (size_t)(ry0 + yy) * pitch + rx0;
-        for (int xx = lane; xx < w; xx += 32) smem[xx * cs + yy] = __ldg(row + xx);
-    }
-}
-
-struct SmemPlan {
-    int region_floats;  // staged region
-    int estride;        // floats per block error table (== 8 mod 32)
-    size_t bytes;
-};
-
-__host__ __device__ inline int error_table_floats(const StackJob& job) {
-    const int ws = 2 * job.bm_range + 1, wt = 2 * job.ps_range + 1;
-    const int spatial = (ws * ws + 3) & ~3;
-    const int temporal = job.radius > 0 ? job.ps_num * ((wt * wt + 3) & ~3) : 0;
-    return spatial > temporal ? spatial : temporal;
-}
-
-__host__ __device__ inline SmemPlan smem_plan(const StackJob& job) {
-    SmemPlan p;
-    const int reach = job.bm_range + job.radius * job.ps_range;
-    const int tile_w = (kTileBX - 1) * job.step + 8, tile_h = (kTileBY - 1) * job.step + 8;
-    const int w = tile_w + 2 * reach < job.width ? tile_w + 2 * reach : job.width;
-    const int h = tile_h + 2 * reach < job.height ? tile_h + 2 * reach : job.height;
-    const int cs = (h + kMaxK + 7) | 1;
-    p.region_floats = cs * w;
-    p.estride = ((error_table_floats(job) + 31) & ~31) + 8;
-    p.bytes = sizeof(float) * (size_t(kGroups) * 64 + size_t(kGroups) * p.estride + p.region_floats) +
-              sizeof(Window) * kGroups * 8 + sizeof(GroupState) * kGroups;
-    return p;
 }
 
 }  // namespace
 
-// Shared memory: block state, windows, reference blocks, error tables, then
-// the staged region.
-__global__ void __launch_bounds__(kMatchThreads, 1) bm3d_match_sliding_kernel(const StackJob job) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const SmemPlan plan = smem_plan(job);
-    GroupState* gs_all = reinterpret_cast<GroupState*>(smem_raw);
-    Window* win_all = reinterpret_cast<Window*>(gs_all + kGroups);
-    float* cur_all = reinterpret_cast<float*>(win_all + kGroups * 8);
-    float* etab_all = cur_all + kGroups * 64;
-    float* region = etab_all + (size_t)kGroups * plan.estride;
-
-    const int lane = threadIdx.x & 31;
-    const int sub = lane & 7;
-    const int g = threadIdx.x >> 3;         // group in the CTA
-    const int wrp = g >> 2, gi = g & 3;     // warp, group in the warp
-    const unsigned gmask = 0xffu << (lane & ~7);
-    const int tiles_x = (job.nbx + kTileBX - 1) / kTileBX;
-    const int tx = blockIdx.x % tiles_x, ty = blockIdx.x / tiles_x;
-    const int bx0 = tx * kTileBX, by0 = ty * kTileBY;
-    const int bx_last = min(bx0 + kTileBX - 1, job.nbx - 1);
-    const int by_last = min(by0 + kTileBY - 1, job.nby - 1);
-    // warp wrp: block row wrp/2, block columns (wrp&1) + {0, 2, 4, 6}
-    const int bxr = bx0 + (wrp & 1) + 2 * gi, byr = by0 + (wrp >> 1);
-    const bool valid = bxr < job.nbx && byr < job.nby;
-    const int bx = min(bxr, job.nbx - 1), by = min(byr, job.nby - 1);
-    const int W = job.width, H = job.height;
-    const int x = min(bx * job.step, W - 8);
-    const int y = min(by * job.step, H - 8);
-    const int tile_x0 = min(bx0 * job.step, W - 8), tile_x1 = min(bx_last * job.step, W - 8);
-    const int tile_y0 = min(by0 * job.step, H - 8), tile_y1 = min(by_last * job.step, H - 8);
-    const int r = job.radius;
-    const int R = job.bm_range, Q = job.ps_range, P = job.ps_num;
-    const int pitch = job.pitch;
-
-    float* cur_s = cur_all + g * 64;
-    float* E = etab_all + (size_t)g * plan.estride;
-    Window* win = win_all + g * 8;
-    GroupState* gs = gs_all + g;
-    const float* fc = job.slice_frame[r];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) cur_s[sub * 8 + i] = __ldg(fc + (size_t)(y + i) * pitch + x + sub);
-    __syncwarp(gmask);
-    float c7[8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i) c7[i] = cur_s[56 + i];
-
-    auto stage = [&](const float* frame, int reach) {
-        Region s;
-        const int rx0 = max(tile_x0 - reach, 0);
-        const int rx1 = min(tile_x1 + reach, W - 8) + 7;
-        const int ry0 = max(tile_y0 - reach, 0);
-        const int ry1 = min(tile_y1 + reach, H - 8) + 7;
-        // column: the region's rows plus the rows masked chunk rows may read
-        s.cs = (ry1 - ry0 + 1 + kMaxK + 7) | 1;
-        s.rx0 = rx0;
-        s.ry0 = ry0;
-        s.rx1 = rx1;
-        s.ry1 = ry1;
-        s.smem = region;
-        __syncthreads();  // the previous phase has finished with the region
-        stage_region(region, frame, pitch, rx0, ry0, rx1, ry1, s.cs);
-        __syncthreads();
-        return s;
-    };
-
-    // spatial search (src/bm3d.comp:479-538)
-    {
-        const Region s = stage(fc, R);
-        if (sub == 0) win[0] = make_window(x, y, R, W, H, 0, 0);
-        __syncwarp(gmask);
-        search_windows(s, cur_s, c7, win, 1, E, gs, gmask, job.status);
-        const uint64_t k = gs->top[sub];
-        const uint32_t xy = key_xy(k, win, 0);
-        gs->ge[sub] = key_err(k);
-        gs->gxy[sub] = xy;
-        gs->gz[sub] = r;
-        gs->sxy[sub] = xy;
-        __syncwarp(gmask);
-    }
-
-    // temporal predictive search (src/bm3d.comp:540-637)
-    const int area = (2 * Q + 1) * (2 * Q + 1);
-    for (int dir = -1; dir <= 1; dir += 2) {
-        gs->pxy[sub] = gs->sxy[sub];
-        __syncwarp(gmask);
-        for (int t = 1; t <= r; ++t) {
-            const int z = r + dir * t;
-            const Region s = stage(job.slice_frame[z], R + t * Q);
-            if (sub == 0) {
-                int eoff = 0;
-                for (int i = 0; i < P; ++i) {
-                    const uint32_t p = gs->pxy[i];
-                    win[i] = make_window(int(p & 0xffffu), int(p >> 16), Q, W, H, i * area, eoff);
-                    eoff += (win[i].rw * win[i].h + 3) & ~3;  // tables start 4-aligned
-                }
-            }
-            __syncwarp(gmask);
-            search_windows(s, cur_s, c7, win, P, E, gs, gmask, job.status);
-            if (sub == 0) {
-                for (int i = 0; i < P; ++i) {
-                    const uint64_t k = gs->top[i];
-                    const uint32_t fxy = key_xy(k, win, area);
-                    ginsert(gs->ge, gs->gxy, gs->gz, key_err(k), fxy, z);
-                    gs->pxy[i] = fxy;
-                }
-            }
-            __syncwarp(gmask);
-        }
-    }
-
-    if (valid && sub == 0) {
-        // forced self-match (src/bm3d.comp:639-663)
-        uint32_t gxy[8];
-        int gz[8];
-        for (int k = 0; k < 8; ++k) {
-            gxy[k] = gs->gxy[k];
-            gz[k] = gs->gz[k];
-        }
-        const uint32_t self_xy = uint32_t(x) | (uint32_t(y) << 16);
-        bool has_self = false;
-        for (int k = 0; k < 8; ++k) has_self = has_self || (gxy[k] == self_xy && gz[k] == r);
-        if (!has_self) {
-            for (int k = 7; k > 0; --k) {
-                gxy[k] = gxy[k - 1];
-                gz[k] = gz[k - 1];
-            }
-            gxy[0] = self_xy;
-            gz[0] = r;
-        }
-        const size_t b = (size_t)by * job.nbx + bx;
-        uint4* dst = reinterpret_cast<uint4*>(job.match_xy + b * 8);
-        dst[0] = make_uint4(gxy[0], gxy[1], gxy[2], gxy[3]);
-        dst[1] = make_uint4(gxy[4], gxy[5], gxy[6], gxy[7]);
-        uint32_t zp = 0;
-        for (int k = 0; k < 8; ++k) zp |= uint32_t(gz[k]) << (4 * k);
-        job.match_z[b] = zp;
-    }
+const char* tile_shape_name(TileShape shape) {
+    static const char* names[kTileShapes] = {"8x4", "16x2", "4x8", "8x2", "4x4"};
+    return (shape >= 0 && shape < kTileShapes) ? names[shape] : "?";
 }
 
-namespace {
-constexpr size_t kSmemBudget = 220 * 1024;
+size_t tile_smem_bytes(const StackJob& job, TileShape shape, TileMode mode) {
+    return plan_bytes(job, shape, mode);
 }
 
-// True when the tiled kernel handles this configuration: its shared memory
-// fits, and every temporal window is centred on a real match. (A corner
-// block's spatial window holds (min(R, W-8)+1) * (min(R, H-8)+1) candidates;
-// with fewer than ps_num of them the reference seeds a temporal window at
-// (0, 0), which can lie outside the tile's staged region.) Otherwise the
-// caller uses the direct-read kernel.
-bool match_sliding_fits(const StackJob& job) {
-    if (smem_plan(job).bytes > kSmemBudget) return false;
+int tile_count(const StackJob& job, TileShape shape) {
+    const ShapeInfo si = kShapes[shape];
+    return ((job.nbx + si.tx - 1) / si.tx) * ((job.nby + si.ty - 1) / si.ty);
+}
+
+// True when the tiled kernel handles this configuration with this shape:
+// radius < 3 (the sliding scan), its shared memory fits, and every temporal
+// window is centred on a real match. (A corner block's spatial window holds
+// (min(R, W-8)+1) * (min(R, H-8)+1) candidates; with fewer than ps_num of
+// them the reference seeds a temporal window at (0, 0), which can lie
+// outside the tile's staged region.) Otherwise the caller uses the
+// direct-read kernel.
+bool tile_shape_fits(const StackJob& job, TileShape shape, TileMode mode) {
+    if (job.radius >= 3) return false;
+    if (plan_bytes(job, shape, mode) > kSmemBudget) return false;
     if (job.radius > 0) {
         const int cw = std::min(job.bm_range, job.width - 8) + 1;
         const int ch = std::min(job.bm_range, job.height - 8) + 1;
@@ -584,14 +71,35 @@ bool match_sliding_fits(const StackJob& job) {
     return true;
 }
 
-cudaError_t launch_match_sliding(const StackJob& job, cudaStream_t stream) {
-    const size_t smem = smem_plan(job).bytes;
-    cudaError_t e = cudaFuncSetAttribute(bm3d_match_sliding_kernel,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    const int tiles = ((job.nbx + kTileBX - 1) / kTileBX) * ((job.nby + kTileBY - 1) / kTileBY);
-    bm3d_match_sliding_kernel<<<tiles, kMatchThreads, smem, stream>>>(job);
-    return cudaGetLastError();
+// The default shape of the plain path: the first that fits, largest tiles
+// first.
+int default_tile_shape(const StackJob& job, TileMode mode) {
+    const TileShape order[] = {kTile8x4, kTile16x2, kTile8x2, kTile4x4};
+    for (TileShape s : order)
+        if (tile_shape_fits(job, s, mode)) return s;
+    return -1;
+}
+
+cudaError_t launch_match_tiles(const StackJob& job, TileShape shape, TileMode mode,
+                               cudaStream_t stream) {
+    switch (shape) {
+        case kTile8x4: return launch_tiles_8x4(job, mode, stream);
+        case kTile16x2: return launch_tiles_16x2(job, mode, stream);
+        case kTile4x8: return launch_tiles_4x8(job, mode, stream);
+        case kTile8x2: return launch_tiles_8x2(job, mode, stream);
+        default: return launch_tiles_4x4(job, mode, stream);
+    }
+}
+
+cudaError_t launch_batch_tiles(const BatchWork& work, TileShape shape, TileMode mode, size_t smem,
+                               int grid, cudaStream_t stream) {
+    switch (shape) {
+        case kTile8x4: return launch_batch_8x4(work, mode, smem, grid, stream);
+        case kTile16x2: return launch_batch_16x2(work, mode, smem, grid, stream);
+        case kTile4x8: return launch_batch_4x8(work, mode, smem, grid, stream);
+        case kTile8x2: return launch_batch_8x2(work, mode, smem, grid, stream);
+        default: return launch_batch_4x4(work, mode, smem, grid, stream);
+    }
 }
 
 }  // namespace vsfeel

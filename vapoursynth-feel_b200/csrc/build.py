@@ -17,8 +17,10 @@ CSRC = Path(__file__).resolve().parent
 PKG = CSRC.parent / "vsfeel"
 INCLUDE = CSRC.parent.parent / "include"
 LIB = PKG / "libvsfeel_bm3d.so"
-SOURCES = ["bm3d_kernels.cu", "bm3d_match.cu", "bm3d_engine.cu", "bm3d_noalloc.cu"]
-HEADERS = ["bm3d_device.cuh"]
+SOURCES = ["bm3d_kernels.cu", "bm3d_match.cu", "bm3d_match_8x4.cu", "bm3d_match_16x2.cu",
+           "bm3d_match_4x8.cu", "bm3d_match_8x2.cu", "bm3d_match_4x4.cu", "bm3d_engine.cu",
+           "bm3d_noalloc.cu", "bm3d_batch.cu"]
+HEADERS = ["bm3d_device.cuh", "bm3d_filter.cuh", "bm3d_match.cuh"]
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
@@ -39,20 +41,26 @@ def _stale() -> bool:
 def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not _stale():
         return LIB
-    objs = []
     build_dir = CSRC / "_build"
     build_dir.mkdir(exist_ok=True)
-    for src in SOURCES:
+
+    def compile_one(src):
         obj = build_dir / (Path(src).stem + ".o")
         cmd = [NVCC, *FLAGS, "-c", str(CSRC / src), "-o", str(obj)]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        proc = subprocess.run(cmd, capture_output=True, text=True)
-        if proc.returncode != 0:
-            raise RuntimeError(f"nvcc failed on {src}:\n{proc.stdout}\n{proc.stderr}")
-        if verbose:
-            sys.stderr.write(proc.stderr)
-        objs.append(str(obj))
+        return src, obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    from concurrent.futures import ThreadPoolExecutor
+
+    objs = []
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as pool:
+        for src, obj, proc in pool.map(compile_one, SOURCES):
+            if proc.returncode != 0:
+                raise RuntimeError(f"nvcc failed on {src}:\n{proc.stdout}\n{proc.stderr}")
+            if verbose:
+                sys.stderr.write(proc.stderr)
+            objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")
     proc = subprocess.run([NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a",
                            *objs, "-o", str(tmp), "-lcudart_static", "-lrt", "-lpthread", "-ldl"],

@@ -31,6 +31,12 @@ EXPORTS = (
     "vsfeel_bm3d_saved_layout",
     "vsfeel_bm3d_forward_saved",
     "vsfeel_bm3d_backward",
+    "vsfeel_bm3d_batch_create",
+    "vsfeel_bm3d_batch_run",
+    "vsfeel_bm3d_batch_finish",
+    "vsfeel_bm3d_batch_classes",
+    "vsfeel_bm3d_batch_class",
+    "vsfeel_bm3d_batch_free",
     "vsfeel_bm3d_process_device_noalloc",
     "vsfeel_bm3d_noalloc_scratch_bytes",
     "vsfeel_bm3d_last_error",
@@ -107,6 +113,32 @@ class SavedInfo(ctypes.Structure):
         "den_offset", "den_row_stride", "den_frame_stride", "num_blocks")]
 
 
+BATCH_AUTOTUNE = 1
+TILE_SHAPES = ("8x4", "16x2", "4x8", "8x2", "4x4")
+
+
+class BatchClip(ctypes.Structure):
+    _fields_ = [
+        ("args", Args),
+        ("width", ctypes.c_int), ("height", ctypes.c_int), ("num_frames", ctypes.c_int),
+        ("src", ctypes.c_void_p),
+        ("src_frame_stride", ctypes.c_int64), ("src_row_stride", ctypes.c_int64),
+        ("dst", ctypes.c_void_p),
+        ("dst_frame_stride", ctypes.c_int64), ("dst_row_stride", ctypes.c_int64),
+    ]
+
+
+class BatchClassInfo(ctypes.Structure):
+    _fields_ = [
+        ("radius", ctypes.c_int), ("block_step", ctypes.c_int), ("bm_range", ctypes.c_int),
+        ("ps_num", ctypes.c_int), ("ps_range", ctypes.c_int),
+        ("clips", ctypes.c_int), ("stacks", ctypes.c_int),
+        ("tiles", ctypes.c_int64),
+        ("tile_shape", ctypes.c_int),
+        ("tuned_ms", ctypes.c_double * len(TILE_SHAPES)),
+    ]
+
+
 FETCH_FN = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                             ctypes.POINTER(ctypes.c_ssize_t))
 RELEASE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int)
@@ -159,6 +191,19 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.vsfeel_bm3d_forward_saved.restype = c_int
     lib.vsfeel_bm3d_backward.argtypes = [c_p, c_p, c_p, c_i64, c_i64, c_p, c_i64, c_i64, c_p]
     lib.vsfeel_bm3d_backward.restype = c_int
+    lib.vsfeel_bm3d_batch_create.argtypes = [ctypes.POINTER(BatchClip), c_int, c_int, c_int,
+                                             ctypes.POINTER(c_p)]
+    lib.vsfeel_bm3d_batch_create.restype = c_int
+    lib.vsfeel_bm3d_batch_run.argtypes = [c_p, c_p]
+    lib.vsfeel_bm3d_batch_run.restype = c_int
+    lib.vsfeel_bm3d_batch_finish.argtypes = [c_p]
+    lib.vsfeel_bm3d_batch_finish.restype = c_int
+    lib.vsfeel_bm3d_batch_classes.argtypes = [c_p, ctypes.POINTER(c_int), ctypes.POINTER(c_i64)]
+    lib.vsfeel_bm3d_batch_classes.restype = c_int
+    lib.vsfeel_bm3d_batch_class.argtypes = [c_p, c_int, ctypes.POINTER(BatchClassInfo)]
+    lib.vsfeel_bm3d_batch_class.restype = c_int
+    lib.vsfeel_bm3d_batch_free.argtypes = [c_p]
+    lib.vsfeel_bm3d_batch_free.restype = None
     lib.vsfeel_bm3d_process_device_noalloc.argtypes = [ctypes.POINTER(Args),
                                                        ctypes.POINTER(VideoInfo), c_p, c_i64,
                                                        c_i64, c_p, c_i64, c_i64, c_int, c_int, c_p]

@@ -67,6 +67,21 @@ class Denoiser:
         if t.device.index != self.device:
             raise Error(f"BM3D: {name} is on {t.device}, the context on cuda:{self.device}")
 
+    def plain(self, x, out=None):
+        """The plain forward pass (no saved state) into out, on torch's
+        current stream."""
+        import torch
+
+        self._validate(x, "input")
+        if out is None:
+            out = torch.empty(self.shape, dtype=torch.float32, device=x.device)
+        self._validate(out, "output")
+        stream = torch.cuda.current_stream(x.device).cuda_stream
+        self._check(self.lib.vsfeel_bm3d_process_device(
+            self.handle, x.data_ptr(), x.stride(0), x.stride(1), out.data_ptr(), out.stride(0),
+            out.stride(1), 0, self.shape[0], stream))
+        return out
+
     def forward_saved(self, x):
         """(output, saved) for x; saved is a uint8 CUDA tensor of the frozen state."""
         import torch

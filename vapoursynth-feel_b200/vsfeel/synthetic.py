@@ -68,3 +68,24 @@ def make_chroma(nframes: int, height: int, width: int, seed: int = 0) -> np.ndar
         out[f] = 0.5 + 0.4 * np.sin(
             2.0 * np.pi * (xx * np.cos(theta) + yy * np.sin(theta)) / period + phase)
     return out
+
+
+def make_clip_device(nframes: int, height: int, width: int, sigma: float = 3.0, shift: int = 3,
+                     seed: int = 0, device="cuda"):
+    """make_clip's recipe with the frames built on the GPU (for large
+    benchmark batches): the canvas and the per-frame offsets come from the
+    same numpy draws as make_clip; the noise comes from torch's generator
+    seeded with `seed`, so the noise values differ from make_clip's."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    canvas = torch.from_numpy(
+        clean_canvas(rng, height + 2 * shift, width + 2 * shift).astype(np.float32)).to(device)
+    gen = torch.Generator(device=device).manual_seed(int(seed))
+    out = torch.empty((nframes, height, width), dtype=torch.float32, device=device)
+    for f in range(nframes):
+        dx, dy = (int(v) for v in rng.integers(-shift, shift + 1, size=2))
+        out[f] = canvas[shift + dy:shift + dy + height, shift + dx:shift + dx + width]
+        if sigma > 0:
+            out[f] += torch.randn((height, width), generator=gen, device=device) * (sigma / 255.0)
+    return out
