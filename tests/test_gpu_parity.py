@@ -193,3 +193,14 @@ def test_kernels_launched_through_native_library():
     node = _node(frames, radius=1)
     node.output()
     assert node._ctx.lib.vsfeel_bm3d_launch_count(node._ctx.handle) > 0
+
+
+def test_frame_shards_match_whole_clip():
+    from vsfeel import shard
+
+    params = dict(sigma=6.0, block_step=4, bm_range=8, radius=2, ps_num=2, ps_range=3)
+    frames = make_clip(9, 64, 80, sigma=6.0, shift=3, seed=41)
+    whole = _node(frames, **params).output()
+    parts = [shard.denoise_shard(frames, s, shard.cuda_denoiser(params))
+             for s in shard.plan(9, 3, params["radius"])]
+    assert float(np.abs(np.concatenate(parts) - whole).max()) <= TYPICAL_TOL
