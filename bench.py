@@ -163,6 +163,10 @@ GRAD_WORKLOADS = {
     # the plain workload's clip and settings, forward + backward
     "fwd_bwd_1920x1080x32_r2": dict(frames=32, height=HEIGHT, width=WIDTH, shift=4, seed=2000,
                                     params=dict(PARAMS)),
+    # the large workload: 24 frames 3840x2160, radius 4 (true 8x8 SSD search)
+    "fwd_bwd_3840x2160x24_r4": dict(frames=24, height=2160, width=3840, shift=6, seed=4000,
+                                    params=dict(sigma=8.0, block_step=4, bm_range=16, radius=4,
+                                                ps_num=4, ps_range=7, extractor_exp=2)),
 }
 
 
@@ -172,20 +176,20 @@ def time_fwd_bwd(torch, dev, name, steps, warmup):
     sum(W * out) with W ~ N(0, 1) seeded."""
     import vsfeel
     from vsfeel.autograd import Denoiser
-    from vsfeel.synthetic import make_clip
+    from vsfeel.synthetic import make_clip_device
 
     wl = GRAD_WORKLOADS[name]
     n, h, w = wl["frames"], wl["height"], wl["width"]
-    frames = make_clip(n, h, w, sigma=wl["params"]["sigma"], shift=wl["shift"], seed=wl["seed"])
-    x = torch.from_numpy(frames).to(dev)
+    x = make_clip_device(n, h, w, sigma=wl["params"]["sigma"], shift=wl["shift"], seed=wl["seed"],
+                         device=dev)
     weights = torch.randn(x.shape, generator=torch.Generator(device=dev).manual_seed(6),
                           device=dev)
-    node = vsfeel.BM3Dv2(vsfeel.clip_from_array(frames), device=dev.index, **wl["params"])
     den = Denoiser(x.shape, dev.index, **wl["params"])
+    fwd_den = Denoiser(x.shape, dev.index, **wl["params"])
     plain = torch.empty_like(x)
 
     def fwd():
-        node.output_device(x, plain)
+        fwd_den.plain(x, plain)
 
     def fwd_bwd():
         xr = x.detach().requires_grad_(True)
@@ -205,10 +209,12 @@ def time_fwd_bwd(torch, dev, name, steps, warmup):
         torch.cuda.synchronize()
         return a.elapsed_time(b) / steps
 
-    torch.cuda.reset_peak_memory_stats(dev)
-    free0, total = torch.cuda.mem_get_info(dev)
     fwd_ms = timed(fwd)
+    fwd_den.close()
+    torch.cuda.synchronize()
+    torch.cuda.reset_peak_memory_stats(dev)
     fb_ms = timed(fwd_bwd)
+    torch_peak = int(torch.cuda.max_memory_allocated(dev))
     # adjoint kernel alone
     out, saved = den.forward_saved(x)
     torch.cuda.synchronize()
@@ -217,8 +223,9 @@ def time_fwd_bwd(torch, dev, name, steps, warmup):
     return {"workload": name, "fwd_mpx_s": px / fwd_ms / 1e3, "fwd_bwd_mpx_s": px / fb_ms / 1e3,
             "fwd_ms": fwd_ms, "fwd_bwd_ms": fb_ms, "backward_only_ms": adj_ms,
             "fwd_bwd_over_fwd": fb_ms / fwd_ms, "saved_state_bytes": int(den.layout.bytes),
-            "torch_peak_bytes": int(torch.cuda.max_memory_allocated(dev)),
-            "library_bytes": int(den.info.device_bytes + node.info.device_bytes),
+            "peak_hbm_bytes_fwd_bwd": torch_peak + int(den.info.device_bytes),
+            "peak_hbm_note": "torch's peak allocation during forward+backward (clip, output, "
+                             "saved state, gradients) plus the library context's buffers",
             "steps": steps, "warmup": warmup}
 
 
@@ -484,7 +491,8 @@ def main() -> int:
         "clocks": clk,
     }
     if world == 1 and not args.no_grad:
-        line["fwd_bwd"] = [time_fwd_bwd(torch, dev, name, max(3, args.steps // 2), 3)
+        line["fwd_bwd"] = [time_fwd_bwd(torch, dev, name,
+                                        3 if name.endswith("_r4") else max(3, args.steps // 2), 3)
                            for name in GRAD_WORKLOADS]
     if world == 1 and not args.no_batch:
         line["batched"] = time_batched(torch, dev, max(2, args.steps // 3), 3)

@@ -80,6 +80,9 @@ class Oracle:
         lib.oracle_bm3d_f64.restype = _i
         lib.oracle_bm3d_matches_f32.argtypes = [_p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i, _i, _p]
         lib.oracle_bm3d_matches_f32.restype = _i
+        lib.oracle_bm3d_final.argtypes = [_p, _p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i, _i,
+                                          _i, _i, _i, _p]
+        lib.oracle_bm3d_final.restype = _i
         lib.oracle_bm3d_frozen_state.argtypes = [_p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i,
                                                  _i, _i, _p, _p]
         lib.oracle_bm3d_frozen_state.restype = _i
@@ -100,11 +103,23 @@ class Oracle:
         self.lib = lib
 
     def bm3d(self, frames, params: Params, out_first=0, out_count=None, nthreads=None,
-             fp64=False) -> np.ndarray:
+             fp64=False, ref=None) -> np.ndarray:
+        """ref: the basic estimate; given, runs the final (Wiener) pass."""
         a = _frames(frames)
         n, h, w = a.shape
         out_count = n - out_first if out_count is None else out_count
         out = np.empty((out_count, h, w), dtype=np.float64 if fp64 else np.float32)
+        if ref is not None:
+            r = _frames(ref)
+            if r.shape != a.shape:
+                raise ValueError("ref must have the clip's shape")
+            rc = self.lib.oracle_bm3d_final(_ptr(a), _ptr(r), n, w, h, *params.args(),
+                                            params.extractor_exp, out_first, out_count,
+                                            nthreads or _default_threads(), 1 if fp64 else 0,
+                                            _ptr(out))
+            if rc != 0:
+                raise ValueError("oracle rejected the arguments")
+            return out
         fn = self.lib.oracle_bm3d_f64 if fp64 else self.lib.oracle_bm3d_f32
         rc = fn(_ptr(a), n, w, h, *params.args(), params.extractor_exp, out_first, out_count,
                 nthreads or _default_threads(), _ptr(out))
@@ -178,7 +193,8 @@ class ReferenceShaders:
             if build.build_ref() is None:
                 raise FileNotFoundError("reference shaders are not built (no reference tree)")
         lib = ctypes.CDLL(str(path))
-        lib.ref_bm3d_clip.argtypes = [_p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i, _i, _i, _i, _p]
+        lib.ref_bm3d_clip.argtypes = [_p, _p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i, _i, _i, _i,
+                                      _p]
         lib.ref_bm3d_clip.restype = _i
         lib.ref_bm3d_stack.argtypes = [_p, _i, _i, _i, _f, _i, _i, _i, _i, _i, _i, _i, _i, _p]
         lib.ref_bm3d_stack.restype = _i
@@ -204,13 +220,19 @@ class ReferenceShaders:
     def available(cls) -> bool:
         return cls.PATH.exists()
 
-    def bm3d(self, frames, params: Params, out_first=0, out_count=None, nthreads=1) -> np.ndarray:
+    def bm3d(self, frames, params: Params, out_first=0, out_count=None, nthreads=1,
+             ref=None) -> np.ndarray:
+        """ref: the basic estimate for the final (Wiener) pass."""
         a = _frames(frames)
         n, h, w = a.shape
         out_count = n - out_first if out_count is None else out_count
         out = np.empty((out_count, h, w), dtype=np.float32)
         p = params
-        rc = self.lib.ref_bm3d_clip(_ptr(a), n, w, h, _f(p.sigma), p.block_step, p.bm_range,
+        r = None if ref is None else _frames(ref)
+        if r is not None and r.shape != a.shape:
+            raise ValueError("ref must have the clip's shape")
+        rc = self.lib.ref_bm3d_clip(_ptr(a), None if r is None else _ptr(r), n, w, h, _f(p.sigma),
+                                    p.block_step, p.bm_range,
                                     p.radius, p.ps_num, p.ps_range, p.extractor_exp, out_first,
                                     out_count, nthreads, _ptr(out))
         if rc != 0:

@@ -44,9 +44,10 @@ namespace {
 
 struct Params {
     int width, height, stride, nframes;
-    double thr;        // sigma * hard-pass factor, src/bm3d.cpp:1103-1113
+    double thr;        // SIGMA_Y: sigma * the pass's factor, src/bm3d.cpp:1103-1113
     int step, bm_range, radius, ps_num, ps_range;
     double extractor;  // ldexp(1, exp) or 0, src/bm3d.cpp:1188-1190
+    bool final_pass;   // Wiener pass with a "ref" clip, src/bm3d.cpp:1062-1083
 };
 
 inline int clampi(int v, int lo, int hi) { return std::min(std::max(v, lo), hi); }
@@ -278,10 +279,12 @@ void ginsert8(T ge[8], int gx[8], int gy[8], int gz[8], T err, int cx, int cy, i
 }
 
 struct Frames {
-    const float* base;  // nframes planes of height*stride floats
+    const float* base;  // the search clip: nframes planes of height*stride floats
     size_t plane;
     int nframes;
+    const float* input = nullptr;  // the denoised clip in the final pass (else base)
     const float* at(int f) const { return base + (size_t)f * plane; }
+    const float* input_at(int f) const { return (input ? input : base) + (size_t)f * plane; }
 };
 
 // The 8 matches (x, y, z) of the reference block at (x, y) of stack m,
@@ -425,10 +428,70 @@ T filter_group(const Params& P, T X[8][8][8], uint64_t* keep_bits = nullptr) {
     return weight;
 }
 
+// Collaborative Wiener filtering, the final pass (src/bm3d.comp:401-443):
+// the 3D transform of the group (X) and of the basic estimate's group at the
+// same positions (Xr), coefficient r^2 / (r^2 + SIGMA_Y^2) per coefficient
+// (1 at DC), the product scaled by 1/4096, weight 1 / sum(coefficient^2),
+// inverse transform of X. Per coefficient, rr = r*r and SS = SIGMA_Y*SIGMA_Y
+// are rounded products and rr + SS is an unfused sum (SIGMA_Y is a
+// specialisation constant, so a shader compiler folds SS), while the
+// accumulation ks += coeff*coeff is fused like the other "a += b*c"
+// statements. The sums of the squared coefficients follow the reference's
+// order: per horizontal frequency b, four partial sums by vertical frequency
+// mod 4 over (group frequency, vertical frequency), then
+// (ks0 + ks1) + (ks2 + ks3), then the pairwise tree over b
+// (src/bm3d.comp:238-246).
+template <class T>
+void transform3(T X[8][8][8], bool inverse) {
+    T v[8];
+    for (int k = 0; k < 8; ++k)
+        for (int b = 0; b < 8; ++b) {
+            for (int a = 0; a < 8; ++a) v[a] = X[k][a][b];
+            inverse ? dct8_inv(v) : dct8_fwd(v);
+            for (int a = 0; a < 8; ++a) X[k][a][b] = v[a];
+        }
+    for (int k = 0; k < 8; ++k)
+        for (int a = 0; a < 8; ++a) inverse ? dct8_inv(X[k][a]) : dct8_fwd(X[k][a]);
+    for (int a = 0; a < 8; ++a)
+        for (int b = 0; b < 8; ++b) {
+            for (int k = 0; k < 8; ++k) v[k] = X[k][a][b];
+            inverse ? dct8_inv(v) : dct8_fwd(v);
+            for (int k = 0; k < 8; ++k) X[k][a][b] = v[k];
+        }
+}
+
+template <class T>
+T wiener_group(const Params& P, T X[8][8][8], T Xr[8][8][8]) {
+    transform3(X, false);
+    transform3(Xr, false);
+    const T sy = T(P.thr);
+    const T ss = sy * sy;
+    T lane_k[8];
+    for (int b = 0; b < 8; ++b) {
+        T ks[4] = {T(0), T(0), T(0), T(0)};
+        for (int k = 0; k < 8; ++k)
+            for (int a = 0; a < 8; ++a) {
+                const T r = Xr[k][a][b];
+                const T rr = r * r;
+                T coeff = rr / (rr + ss);
+                if (k == 0 && a == 0 && b == 0) coeff = T(1);
+                const T val = X[k][a][b] * coeff;
+                ks[a % 4] = std::fma(coeff, coeff, ks[a % 4]);
+                X[k][a][b] = val * (T(1) / T(4096));
+            }
+        lane_k[b] = (ks[0] + ks[1]) + (ks[2] + ks[3]);
+    }
+    const T k = ((lane_k[0] + lane_k[1]) + (lane_k[2] + lane_k[3])) +
+                ((lane_k[4] + lane_k[5]) + (lane_k[6] + lane_k[7]));
+    transform3(X, true);
+    return T(1) / k;
+}
+
 template <class T>
 struct BlockResult {
     int match[8][3];
     T X[8][8][8];
+    T Xr[8][8][8];  // final pass: the basic estimate's group
     T weight;
     uint64_t keep[8];
 };
@@ -463,13 +526,19 @@ void run_stack(const Params& P, const Frames& F, int m, T* slices, int nthreads,
                     BlockResult<T>& br = res[(size_t)ry * nbx + bx];
                     match_block<T>(P, F, m, x, y, br.match);
                     for (int k = 0; k < 8; ++k) {
-                        const float* f = F.at(clampi(m - r + br.match[k][2], 0, P.nframes - 1));
+                        const int fk = clampi(m - r + br.match[k][2], 0, P.nframes - 1);
+                        const float* f = F.input_at(fk);
+                        const float* fr = F.at(fk);
                         for (int a = 0; a < 8; ++a)
-                            for (int b = 0; b < 8; ++b)
-                                br.X[k][a][b] =
-                                    T(f[(size_t)(br.match[k][1] + a) * P.stride + br.match[k][0] + b]);
+                            for (int b = 0; b < 8; ++b) {
+                                const size_t o =
+                                    (size_t)(br.match[k][1] + a) * P.stride + br.match[k][0] + b;
+                                br.X[k][a][b] = T(f[o]);
+                                if (P.final_pass) br.Xr[k][a][b] = T(fr[o]);
+                            }
                     }
-                    br.weight = filter_group<T>(P, br.X, br.keep);
+                    br.weight = P.final_pass ? wiener_group<T>(P, br.X, br.Xr)
+                                             : filter_group<T>(P, br.X, br.keep);
                 }
             }
         };
@@ -516,10 +585,13 @@ int agg_z(int i, int n, int nframes, int radius) {
 }
 
 template <class T, class O>
-int run_clip(const Params& P, const float* frames, int out_first, int out_count, int nthreads, O* out) {
+int run_clip(const Params& P, const float* frames, int out_first, int out_count, int nthreads, O* out,
+             const float* ref = nullptr) {
     const int N = P.nframes, r = P.radius, tw = 2 * r + 1;
     const size_t plane = (size_t)P.height * P.stride;
-    Frames F{frames, plane, N};
+    // the final pass searches (and takes its coefficients from) the ref clip
+    // and denoises the source clip
+    Frames F{P.final_pass ? ref : frames, plane, N, P.final_pass ? frames : nullptr};
     const int m_lo = clampi(out_first - r, 0, N - 1);
     const int m_hi = clampi(out_first + out_count - 1 + r, 0, N - 1);
     std::vector<T> stacks((size_t)(m_hi - m_lo + 1) * 2 * tw * plane, T(0));
@@ -545,12 +617,14 @@ int run_clip(const Params& P, const float* frames, int out_first, int out_count,
 }
 
 bool make_params(Params& P, int nframes, int width, int height, float sigma, int block_step,
-                 int bm_range, int radius, int ps_num, int ps_range, int extractor_exp) {
+                 int bm_range, int radius, int ps_num, int ps_range, int extractor_exp,
+                 bool final_pass = false) {
     if (nframes <= 0 || width < 8 || height < 8) return false;
     if (sigma < 0.0f || block_step < 1 || block_step > 8 || bm_range <= 0 || radius < 0 ||
         radius > 4 || ps_num < 1 || ps_num > 8 || ps_range <= 0)
         return false;
-    uint32_t bits = 0x3f021bb6u;  // hard-pass sigma factor, src/bm3d.cpp:1103-1113
+    // sigma factor of the pass, src/bm3d.cpp:1103-1113
+    uint32_t bits = final_pass ? 0x3e40c0c1u : 0x3f021bb6u;
     float factor;
     std::memcpy(&factor, &bits, 4);
     P.width = width;
@@ -564,6 +638,7 @@ bool make_params(Params& P, int nframes, int width, int height, float sigma, int
     P.ps_num = ps_num;
     P.ps_range = ps_range;
     P.extractor = extractor_exp != 0 ? double(std::ldexp(1.0f, extractor_exp)) : 0.0;
+    P.final_pass = final_pass;
     return true;
 }
 
@@ -611,6 +686,24 @@ int oracle_bm3d_f64(const float* frames, int nframes, int width, int height, flo
         return -1;
     if (out_first < 0 || out_count < 0 || out_first + out_count > nframes) return -1;
     return run_clip<double, double>(P, frames, out_first, out_count, nthreads, out);
+}
+
+// The final (Wiener) pass: frames is the clip to denoise, ref the basic
+// estimate it is matched on. FP32 or (fp64 != 0) FP64 output.
+int oracle_bm3d_final(const float* frames, const float* ref, int nframes, int width, int height,
+                      float sigma, int block_step, int bm_range, int radius, int ps_num,
+                      int ps_range, int extractor_exp, int out_first, int out_count, int nthreads,
+                      int fp64, void* out) {
+    Params P;
+    if (!ref || !make_params(P, nframes, width, height, sigma, block_step, bm_range, radius,
+                             ps_num, ps_range, extractor_exp, true))
+        return -1;
+    if (out_first < 0 || out_count < 0 || out_first + out_count > nframes) return -1;
+    if (fp64)
+        return run_clip<double, double>(P, frames, out_first, out_count, nthreads,
+                                        static_cast<double*>(out), ref);
+    return run_clip<float, float>(P, frames, out_first, out_count, nthreads,
+                                  static_cast<float*>(out), ref);
 }
 
 // Match table of stack m: nblocks x 8 x (x, y, z), blocks in raster order.

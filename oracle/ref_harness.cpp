@@ -176,11 +176,11 @@ struct Setup {
 };
 
 bool setup(Setup& S, int nframes, int W, int H, float sigma, int step, int R, int r, int P,
-           int Q, int extractor_exp) {
+           int Q, int extractor_exp, bool final_pass = false) {
     if (nframes <= 0 || W < 8 || H < 8 || sigma < 0.0f || step < 1 || step > 8 || R <= 0 ||
         r < 0 || r > 4 || P < 1 || P > 8 || Q <= 0)
         return false;
-    uint32_t bits = 0x3f021bb6u;
+    uint32_t bits = final_pass ? 0x3e40c0c1u : 0x3f021bb6u;  // src/bm3d.cpp:1103-1107
     float factor;
     std::memcpy(&factor, &bits, 4);
     S.W = W;
@@ -195,7 +195,7 @@ bool setup(Setup& S, int nframes, int W, int H, float sigma, int step, int R, in
     S.step = step;
     const double spec[14] = {double(W), double(H),    double(S.stride), double(S.thr), double(step),
                              double(R), double(r),    double(P),        double(Q),     double(S.E),
-                             0.0,       0.0,          double(nframes),  0.0};
+                             0.0,       0.0,          double(nframes),  final_pass ? 1.0 : 0.0};
     for (int id = 0; id < 14; ++id) ref_bm3d_set_spec(id, spec[id]);
     return true;
 }
@@ -237,12 +237,22 @@ void run_stack(const Setup& S, float* res, float* src, int m, size_t res_off, in
     for (auto& t : th) t.join();
 }
 
-std::vector<float> load_frames(const Setup& S, const float* frames) {
-    std::vector<float> src((size_t)S.nframes * S.pe, 0.0f);
+// The source ring with slot = frame index. In the final pass a slot holds
+// [ref][source] (src/bm3d.comp:70-81).
+std::vector<float> load_frames(const Setup& S, const float* frames, const float* ref = nullptr) {
+    const int per_slot = ref ? 2 : 1;
+    std::vector<float> src((size_t)S.nframes * per_slot * S.pe, 0.0f);
     for (int f = 0; f < S.nframes; ++f)
-        for (int y = 0; y < S.H; ++y)
-            std::memcpy(&src[(size_t)f * S.pe + (size_t)y * S.stride],
-                        frames + ((size_t)f * S.H + y) * S.W, sizeof(float) * S.W);
+        for (int y = 0; y < S.H; ++y) {
+            const size_t slot = (size_t)f * per_slot * S.pe + (size_t)y * S.stride;
+            if (ref) {
+                std::memcpy(&src[slot], ref + ((size_t)f * S.H + y) * S.W, sizeof(float) * S.W);
+                std::memcpy(&src[slot + S.pe], frames + ((size_t)f * S.H + y) * S.W,
+                            sizeof(float) * S.W);
+            } else {
+                std::memcpy(&src[slot], frames + ((size_t)f * S.H + y) * S.W, sizeof(float) * S.W);
+            }
+        }
     return src;
 }
 
@@ -252,13 +262,14 @@ extern "C" {
 
 // Denoises out_count frames starting at out_first with the reference shaders.
 // frames: nframes x H x W floats; out: out_count x H x W. Returns 0 or -1.
-int ref_bm3d_clip(const float* frames, int nframes, int W, int H, float sigma, int step, int R,
-                  int r, int P, int Q, int extractor_exp, int out_first, int out_count,
-                  int nthreads, float* out) {
+// ref (optional): the basic-estimate clip of the final (Wiener) pass.
+int ref_bm3d_clip(const float* frames, const float* ref, int nframes, int W, int H, float sigma,
+                  int step, int R, int r, int P, int Q, int extractor_exp, int out_first,
+                  int out_count, int nthreads, float* out) {
     Setup S;
-    if (!setup(S, nframes, W, H, sigma, step, R, r, P, Q, extractor_exp)) return -1;
+    if (!setup(S, nframes, W, H, sigma, step, R, r, P, Q, extractor_exp, ref != nullptr)) return -1;
     if (out_first < 0 || out_count < 0 || out_first + out_count > nframes) return -1;
-    std::vector<float> src = load_frames(S, frames);
+    std::vector<float> src = load_frames(S, frames, ref);
     const int m_lo = clampi(out_first - r, 0, nframes - 1);
     const int m_hi = clampi(out_first + out_count - 1 + r, 0, nframes - 1);
     const size_t stack = (size_t)S.tw * 2 * S.pe;

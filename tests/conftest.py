@@ -44,16 +44,29 @@ def pytest_collection_modifyitems(config, items):
 
 
 def load_golden():
-    """[(name, params dict, input frames, reference output)]"""
+    """Basic-estimate cases: [(name, params dict, input frames, reference output)]"""
     data = np.load(GOLDEN)
     meta = json.loads(bytes(data["meta"]).decode())
     return [(m["name"], m["params"], data[f"{m['name']}/input"], data[f"{m['name']}/output"])
-            for m in meta]
+            for m in meta if not m.get("final")]
+
+
+def load_golden_final():
+    """Final-pass cases: [(name, params dict, input frames, ref frames, reference output)]"""
+    data = np.load(GOLDEN)
+    meta = json.loads(bytes(data["meta"]).decode())
+    return [(m["name"], m["params"], data[f"{m['name']}/input"], data[f"{m['name']}/ref"],
+             data[f"{m['name']}/output"]) for m in meta if m.get("final")]
 
 
 @pytest.fixture(scope="session")
 def golden():
     return load_golden()
+
+
+@pytest.fixture(scope="session")
+def golden_final():
+    return load_golden_final()
 
 
 @pytest.fixture(scope="session")

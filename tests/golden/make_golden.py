@@ -51,6 +51,18 @@ CASES = [
                                   ps_range=2), 2, 20),
 ]
 
+# the final (Wiener) pass: "ref" is the reference's own basic estimate of
+# the same clip
+FINAL_CASES = [
+    ("final_r0", 3, 40, 48, dict(sigma=4.0, block_step=8, bm_range=9, radius=0), 3, 31),
+    ("final_r1", 4, 40, 48, dict(sigma=6.0, block_step=4, bm_range=8, radius=1, ps_num=2,
+                                  ps_range=3), 3, 32),
+    ("final_r2_ext", 5, 36, 44, dict(sigma=10.0, block_step=3, bm_range=6, radius=2, ps_num=2,
+                                      ps_range=3, extractor_exp=2), 3, 33),
+    ("final_r3_exact", 5, 32, 40, dict(sigma=8.0, block_step=4, bm_range=5, radius=3, ps_num=2,
+                                        ps_range=2), 5, 34),
+]
+
 
 def main() -> int:
     ref = ReferenceShaders()
@@ -63,6 +75,16 @@ def main() -> int:
         arrays[f"{name}/input"] = frames
         arrays[f"{name}/output"] = out
         meta.append(dict(name=name, params=p.as_dict()))
+        print(f"{name}: {frames.shape} -> mean {float(out.mean()):.6f}")
+    for name, n, h, w, kw, shift, seed in FINAL_CASES:
+        p = Params(**kw)
+        frames = make_clip(n, h, w, sigma=max(p.sigma, 1.0), shift=shift, seed=seed)
+        basic = ref.bm3d(frames, p, nthreads=1)
+        out = ref.bm3d(frames, p, nthreads=1, ref=basic)
+        arrays[f"{name}/input"] = frames
+        arrays[f"{name}/ref"] = basic
+        arrays[f"{name}/output"] = out
+        meta.append(dict(name=name, params=p.as_dict(), final=True))
         print(f"{name}: {frames.shape} -> mean {float(out.mean()):.6f}")
     arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
     np.savez_compressed(OUT, **arrays)

@@ -51,6 +51,43 @@ def test_oracle_stack_slices_match_reference(oracle_lib):
         assert np.array_equal(a, b), f"stack {m}"
 
 
+def test_oracle_final_pass_matches_golden_vectors_bit_exact(golden_final, oracle_lib):
+    """The final (Wiener) pass: reference shaders' output with the reference's
+    own basic estimate as "ref", reproduced bit for bit."""
+    assert len(golden_final) >= 4
+    for name, params, frames, ref, expected in golden_final:
+        out = oracle_lib.bm3d(frames, Params(**params), nthreads=1, ref=ref)
+        assert np.array_equal(out, expected), f"{name}: oracle differs from the reference"
+
+
+@pytest.mark.skipif(not ReferenceShaders.available(), reason="reference shaders not built")
+@pytest.mark.parametrize("radius,step,bm_range,ps_num,ps_range,ext", [
+    (0, 5, 7, 2, 4, 0), (1, 4, 6, 2, 3, 0), (2, 3, 5, 3, 2, 1), (4, 4, 4, 4, 2, 2),
+])
+def test_oracle_final_pass_matches_reference_shaders(radius, step, bm_range, ps_num, ps_range,
+                                                     ext, oracle_lib):
+    p = Params(sigma=6.0, block_step=step, bm_range=bm_range, radius=radius, ps_num=ps_num,
+               ps_range=ps_range, extractor_exp=ext)
+    frames = make_clip(2 * radius + 2, 30, 37, sigma=p.sigma, shift=3, seed=200 + radius)
+    basic = oracle_lib.bm3d(frames, p, nthreads=2)
+    ref = ReferenceShaders().bm3d(frames, p, nthreads=1, ref=basic)
+    out = oracle_lib.bm3d(frames, p, nthreads=2, ref=basic)
+    assert np.array_equal(out, ref)
+
+
+def test_final_pass_is_finite_and_differs_from_the_basic_estimate(oracle_lib):
+    """The reference's own check of the ref pass (tests/test_bm3dv2.py:165-181):
+    finite, and more than 1e-4 away from the basic estimate."""
+    p = Params(sigma=8.0, block_step=4, bm_range=8, radius=1, ps_num=2, ps_range=3)
+    frames = make_clip(4, 40, 48, sigma=8.0, seed=7)
+    basic = oracle_lib.bm3d(frames, p)
+    final = oracle_lib.bm3d(frames, p, ref=basic)
+    assert np.isfinite(final).all()
+    assert float(np.abs(final - basic).max()) > 1e-4
+    f64 = oracle_lib.bm3d(frames, p, ref=basic, fp64=True)
+    assert float(np.abs(final - f64).max()) < 1e-5
+
+
 def _dct2_ortho(v):
     n = len(v)
     k = np.arange(n)[:, None]

@@ -100,17 +100,29 @@ struct Region {
     int rx1, ry1;  // last staged column and row
 };
 
-// SSD of one column of the block (bc) against w[q..q+7].
+__device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi) {
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+
+// SSD of one column of the block (bc) against w[q..q+7]: the even-row and
+// odd-row sums advance together as one packed pair ({even, odd}) with the
+// sm_100 f32x2 subtract and fused multiply-add, each half rounded exactly as
+// the scalar e += d*d of the reference's two chains.
 template <int K>
 __device__ __forceinline__ float column_ssd_at(const float bc[8], const float w[K + 7], int q) {
-    float ev = 0.0f, od = 0.0f;
+    unsigned long long acc = 0ull;  // {+0.0f, +0.0f}
 #pragma unroll
     for (int i = 0; i < 8; i += 2) {
-        const float d0 = __fsub_rn(bc[i], w[q + i]);
-        ev = __fmaf_rn(d0, d0, ev);
-        const float d1 = __fsub_rn(bc[i + 1], w[q + i + 1]);
-        od = __fmaf_rn(d1, d1, od);
+        unsigned long long d;
+        asm("sub.rn.f32x2 %0, %1, %2;"
+            : "=l"(d)
+            : "l"(pack_f32x2(bc[i], bc[i + 1])), "l"(pack_f32x2(w[q + i], w[q + i + 1])));
+        asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(acc) : "l"(d), "l"(acc));
     }
+    float ev, od;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(ev), "=f"(od) : "l"(acc));
     return __fadd_rn(ev, od);
 }
 
@@ -267,25 +279,42 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
         __syncwarp(gmask);
         const float terr = key_err(tkey);
         const uint32_t tseq = uint32_t(tkey);
-        // a window's table is rw*h contiguous words from a 4-aligned offset:
-        // sweep it four entries per load, 32 per group step
+        // a window's table is rw*h contiguous words from a 4-aligned offset.
+        // A group step covers 32 float4 (128 entries), four loads in flight
+        // per lane; nearly every chunk of 16 entries lies above the bound and
+        // costs one comparison of its minimum (entries past the window in its
+        // last float4 only send a chunk down the exact path, which skips them)
         for (int wi = 0; wi < nwin; ++wi) {
             const Window w = wins[wi];
             const int n_w = w.rw * w.h;
+            const int nq = (n_w + 3) >> 2;
             const float4* tab = reinterpret_cast<const float4*>(E + w.eoff);
-            for (int v = sub; 4 * v < n_w; v += 8) {
-                const float4 q = tab[v];
-                const float ev[4] = {q.x, q.y, q.z, q.w};
+            for (int v0 = 0; v0 < nq; v0 += 32) {
+                float4 q[4];
 #pragma unroll
-                for (int u = 0; u < 4; ++u) {
-                    const int f = 4 * v + u;
-                    if (f < n_w && ev[u] <= terr && ev[u] < kFltMax) {
-                        const int d = f / w.h;
-                        const int row = f - d * w.h;
-                        const uint32_t seq = uint32_t(w.seq_base + row * w.rw + d);
-                        if (ev[u] < terr || seq <= tseq) {
-                            const int pos = atomicAdd(&gs->count, 1);
-                            if (pos < kCollect) gs->buf[pos] = make_key(ev[u], int(seq));
+                for (int k = 0; k < 4; ++k) {
+                    const int v = v0 + sub + 8 * k;
+                    q[k] = v < nq ? tab[v] : make_float4(kFltMax, kFltMax, kFltMax, kFltMax);
+                }
+                float mn = kFltMax;
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    mn = fminf(mn, fminf(fminf(q[k].x, q[k].y), fminf(q[k].z, q[k].w)));
+                if (!(mn <= terr)) continue;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float ev[4] = {q[k].x, q[k].y, q[k].z, q[k].w};
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int f = 4 * (v0 + sub + 8 * k) + u;
+                        if (f < n_w && ev[u] <= terr && ev[u] < kFltMax) {
+                            const int d = f / w.h;
+                            const int row = f - d * w.h;
+                            const uint32_t seq = uint32_t(w.seq_base + row * w.rw + d);
+                            if (ev[u] < terr || seq <= tseq) {
+                                const int pos = atomicAdd(&gs->count, 1);
+                                if (pos < kCollect) gs->buf[pos] = make_key(ev[u], int(seq));
+                            }
                         }
                     }
                 }
