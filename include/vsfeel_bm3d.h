@@ -107,6 +107,20 @@ VSFEEL_API int vsfeel_bm3d_get_frame(vsfeel_bm3d* ctx, int n, vsfeel_fetch_fn fe
                           vsfeel_release_fn release, void* user, float* dst,
                           ptrdiff_t dst_stride_bytes);
 
+/* The final (Wiener) pass, for a context created with a "ref" clip (the
+ * basic estimate): block matching runs on ref, ref's groups give the Wiener
+ * coefficients, and src is the clip denoised (src/bm3d.comp:73-81,
+ * 401-443). The plain entry points reject such a context and the *_ref ones
+ * reject the others. For get_frame_ref, fetch(user, clip, n, stride) returns
+ * frame n of the source (clip 0) or of ref (clip 1), and release(user, clip,
+ * n) hands it back. */
+typedef const float* (*vsfeel_fetch2_fn)(void* user, int clip, int n, ptrdiff_t* stride_bytes);
+typedef void (*vsfeel_release2_fn)(void* user, int clip, int n);
+
+VSFEEL_API int vsfeel_bm3d_get_frame_ref(vsfeel_bm3d* ctx, int n, vsfeel_fetch2_fn fetch,
+                                         vsfeel_release2_fn release, void* user, float* dst,
+                                         ptrdiff_t dst_stride_bytes);
+
 /* Whole clip from host memory: src holds all num_frames luma planes
  * (frame f at src + f*frame_stride_bytes, rows row_stride_bytes apart);
  * writes output frames first .. first+count-1 to dst (same layout, frame 0
@@ -116,6 +130,16 @@ VSFEEL_API int vsfeel_bm3d_process_host(vsfeel_bm3d* ctx, const float* src, ptrd
                              ptrdiff_t dst_frame_stride_bytes, ptrdiff_t dst_row_stride_bytes,
                              int first, int count);
 
+/* process_host for the final pass: ref holds the basic estimate's luma
+ * planes in the same form as src. */
+VSFEEL_API int vsfeel_bm3d_process_host_ref(vsfeel_bm3d* ctx, const float* src,
+                                            ptrdiff_t src_frame_stride_bytes,
+                                            ptrdiff_t src_row_stride_bytes, const float* ref,
+                                            ptrdiff_t ref_frame_stride_bytes,
+                                            ptrdiff_t ref_row_stride_bytes, float* dst,
+                                            ptrdiff_t dst_frame_stride_bytes,
+                                            ptrdiff_t dst_row_stride_bytes, int first, int count);
+
 /* Whole clip already in device memory (strides in floats), enqueued on
  * `stream` (a cudaStream_t, used as given: NULL is the default stream).
  * Returns after the work is enqueued; synchronise the stream before reading
@@ -124,11 +148,20 @@ VSFEEL_API int vsfeel_bm3d_process_device(vsfeel_bm3d* ctx, const float* src, in
                                int64_t src_row_stride, float* dst, int64_t dst_frame_stride,
                                int64_t dst_row_stride, int first, int count, void* stream);
 
+/* process_device for the final pass: ref's rows must have src's stride. */
+VSFEEL_API int vsfeel_bm3d_process_device_ref(vsfeel_bm3d* ctx, const float* src,
+                                              int64_t src_frame_stride, int64_t src_row_stride,
+                                              const float* ref, int64_t ref_frame_stride,
+                                              int64_t ref_row_stride, float* dst,
+                                              int64_t dst_frame_stride, int64_t dst_row_stride,
+                                              int first, int count, void* stream);
+
 /* Effective parameters after defaults and scaling (for callers and tests). */
 typedef struct vsfeel_bm3d_info {
     int width, height, num_frames, radius, block_step, bm_range, ps_num, ps_range, num_streams;
     float sigma;      /* user sigma[0]                                    */
-    float threshold;  /* sigma * 0x3f021bb6 (src/bm3d.cpp:1103-1113)      */
+    float threshold;  /* SIGMA_Y: sigma * 0x3f021bb6, or * 0x3e40c0c1 in the
+                         final pass (src/bm3d.cpp:1103-1113)              */
     float extractor;  /* 2^extractor_exp, or 0 (src/bm3d.cpp:1188-1190)   */
     int blocks_x, blocks_y;
     int64_t device_bytes;  /* device memory held by the context           */

@@ -3,9 +3,10 @@
 * a frame callback that returns no frame -> VSFEEL_E_FETCH, and the context
   stays usable;
 * a callback stride below the width -> VSFEEL_E_ARG;
-* a bounded wait that runs out (VSFEEL_TIMEOUT_MS = 1 ms against ~10 ms of
-  GPU work) -> VSFEEL_E_TIMEOUT, after which the context still works once
-  the limit is back to normal.
+* a bounded wait that runs out (VSFEEL_TIMEOUT_MS = 1 ms against ~15 ms of
+  GPU work, pinned buffers so that the copies do not block the host) ->
+  VSFEEL_E_TIMEOUT, after which the context still works once the limit is
+  back to normal.
 """
 
 from __future__ import annotations
@@ -74,13 +75,27 @@ def test_callback_stride_below_width_is_rejected():
 
 
 def test_bounded_wait_times_out_and_the_context_recovers(monkeypatch):
+    import torch
+
+    # pinned host buffers: the copies are asynchronous, so the bounded wait
+    # runs while the GPU still works on the clip (~15 ms at 1080p radius 2)
     frames = make_clip(5, 1080, 1920, sigma=3.0, seed=5)
     params = dict(sigma=3.0, block_step=4, bm_range=16, radius=2, ps_num=2, ps_range=7)
     node = vsfeel.BM3Dv2(vsfeel.clip_from_array(frames), **params)
+    src = torch.from_numpy(frames).pin_memory()
+    out = torch.empty(frames.shape, dtype=torch.float32).pin_memory()
+    ctx = node._ctx
+
+    def run():
+        return ctx.lib.vsfeel_bm3d_process_host(
+            ctx.handle, src.data_ptr(), src.stride(0) * 4, src.stride(1) * 4, out.data_ptr(),
+            out.stride(0) * 4, out.stride(1) * 4, 0, 5)
+
     monkeypatch.setenv("VSFEEL_TIMEOUT_MS", "1")
-    with pytest.raises(vsfeel.Error, match="timed out after"):
-        node.output()
+    rc = run()
+    assert rc == _lib.E_TIMEOUT
+    assert "timed out after" in _lib.last_error(ctx.lib)
     monkeypatch.delenv("VSFEEL_TIMEOUT_MS")
-    out = node.output(2, 1)
+    assert run() == _lib.OK
     ref = vsfeel.BM3Dv2(vsfeel.clip_from_array(frames), **params).output(2, 1)
-    assert float(np.abs(out - ref).max()) <= 2e-5
+    assert float(np.abs(out.numpy()[2] - ref[0]).max()) <= 2e-5

@@ -22,7 +22,9 @@ constexpr int kSeqSentinel = 0x7fffffff;
 // One stack: the reference blocks of frame m, searched in the slices
 // z = 0..2r (frame clamp(m - r + z)).
 struct StackJob {
-    const float* slice_frame[kMaxTW];  // frame of each slice (search and denoise clip)
+    const float* slice_frame[kMaxTW];  // frame of each slice in the search clip (the clip
+                                       // denoised too, except in the final pass)
+    const float* slice_input[kMaxTW];  // final pass: the same frames of the clip denoised
     float* slice_dst[kMaxTW];          // numerator plane of each slice's target; null = dropped
     int64_t dst_plane;                 // floats from a numerator plane to its weight plane
     int pitch;                         // floats per frame row (inputs)
@@ -30,7 +32,8 @@ struct StackJob {
     int width, height;
     int radius, step, bm_range, ps_num, ps_range;
     int nbx, nby;                      // block grid
-    float thr;                         // hard threshold, sigma * 0x3f021bb6
+    float thr;                         // SIGMA_Y: sigma * 0x3f021bb6 (basic) or 0x3e40c0c1
+    int wiener;                        // final pass: Wiener filter against slice_frame
     float extractor;                   // 2^exp or 0
     uint32_t* match_xy;                // [nblocks][8]: x | y << 16
     uint32_t* match_z;                 // [nblocks]: 8 x 4-bit slice index

@@ -61,8 +61,9 @@ int agg_z(int i, int n, int nframes, int radius) {
     return std::min(std::max(2 * radius - i, n - nframes + 1 + radius), n + radius);
 }
 
-float hard_factor() {
-    const uint32_t bits = 0x3f021bb6u;
+// sigma factor of the pass, src/bm3d.cpp:1103-1107
+float sigma_factor(bool final_pass) {
+    const uint32_t bits = final_pass ? 0x3e40c0c1u : 0x3f021bb6u;
     float f;
     std::memcpy(&f, &bits, 4);
     return f;
@@ -99,6 +100,7 @@ int wait_stream(cudaStream_t s, int64_t limit_ms) {
 struct Settings {
     int width = 0, height = 0, nframes = 0;
     bool chroma = false;
+    bool final_pass = false;  // a "ref" clip was given: the Wiener pass
     float sigma = 3.0f, thr = 0.0f, extractor = 0.0f;
     int step = 8, bm_range = 9, radius = 0, ps_num = 2, ps_range = 4, num_streams = 4;
 };
@@ -175,7 +177,8 @@ int parse_args(const vsfeel_bm3d_args* a, const vsfeel_bm3d_video_info* vi, Sett
     const int ext = a->extractor_exp_set ? a->extractor_exp : 0;
 
     s.sigma = sigma[0];
-    s.thr = sigma[0] * hard_factor();
+    s.final_pass = a->has_ref != 0;
+    s.thr = sigma[0] * sigma_factor(s.final_pass);
     s.extractor = ext != 0 ? std::ldexp(1.0f, ext) : 0.0f;
     s.step = step[0];
     s.bm_range = bmr[0];
@@ -192,9 +195,6 @@ int parse_args(const vsfeel_bm3d_args* a, const vsfeel_bm3d_video_info* vi, Sett
     } else {
         return fail(VSFEEL_E_FORMAT, "only Gray and YUV input are currently supported");
     }
-    if (a->has_ref)
-        return fail(VSFEEL_E_UNSUPPORTED,
-                    "the final (Wiener) pass with \"ref\" is not supported by this build");
     // The reference reads outside the plane below 8x8; the match table packs
     // coordinates in 16 bits.
     if (s.width < 8 || s.height < 8)
@@ -353,13 +353,17 @@ struct vsfeel_bm3d {
 
     // `saved` (the differentiable form): write stack m's match table and keep
     // bits into its record instead of the context's match buffers.
+    // frame_ptr: the search clip (the ref clip in the final pass); input_ptr:
+    // the clip denoised in the final pass (its frames share frame_ptr's pitch)
     void launch_stack(int m, const std::function<const float*(int)>& frame_ptr, int in_pitch,
                       int out_lo, int out_hi, cudaStream_t st, unsigned char* saved = nullptr,
-                      bool table_only = false) {
+                      bool table_only = false,
+                      const std::function<const float*(int)>* input_ptr = nullptr) {
         const int r = s.radius;
         StackJob job{};
         for (int z = 0; z < tw(); ++z) {
             job.slice_frame[z] = frame_ptr(clampf(m - r + z));
+            job.slice_input[z] = input_ptr ? (*input_ptr)(clampf(m - r + z)) : nullptr;
             const int n = clampf(m - r + z);
             job.slice_dst[z] = nullptr;
             if (n >= out_lo && n <= out_hi && read_slice(n, m) == z)
@@ -378,6 +382,7 @@ struct vsfeel_bm3d {
         job.nbx = nbx;
         job.nby = nby;
         job.thr = s.thr;
+        job.wiener = (s.final_pass && input_ptr) ? 1 : 0;
         job.extractor = s.extractor;
         job.match_xy = match_xy.p;
         job.match_z = match_z.p;
@@ -392,8 +397,13 @@ struct vsfeel_bm3d {
         job.status = status_word();
         // fused: one tiled launch matches and filters (the match table stays
         // on chip); otherwise the match table goes through global memory
+        if (table_only) {
+            traced(VSFEEL_KERNEL_MATCH, st, [&] { return launch_match(job, st); });
+            launches += 1;
+            return;
+        }
         const TileMode mode = job.mask_out ? kFusedSave : kFused;
-        const int shape = (fused && table_only == false) ? default_tile_shape(job, mode) : -1;
+        const int shape = (fused && !job.wiener) ? default_tile_shape(job, mode) : -1;
         if (shape >= 0) {
             traced(VSFEEL_KERNEL_MATCH, st,
                    [&] { return launch_match_tiles(job, TileShape(shape), mode, st); });
@@ -433,7 +443,8 @@ struct vsfeel_bm3d {
     // Denoises outputs [first, first+count) from device frames.
     void run(const std::function<const float*(int)>& frame_ptr, int in_pitch,
              const std::function<float*(int)>& out_ptr, int out_pitch, int first, int count,
-             cudaStream_t st, unsigned char* saved = nullptr) {
+             cudaStream_t st, unsigned char* saved = nullptr,
+             const std::function<const float*(int)>* input_ptr = nullptr) {
         if (count <= 0) return;
         const int r = s.radius;
         const int last = first + count - 1;
@@ -449,7 +460,7 @@ struct vsfeel_bm3d {
                 VSF_CUDA(cudaMemsetAsync(slot_pair(n, 0), 0,
                                          sizeof(float) * (size_t)tw() * 2 * acc_plane, st));
             zeroed = std::max(zeroed, want);
-            launch_stack(m, frame_ptr, in_pitch, first, last, st, saved);
+            launch_stack(m, frame_ptr, in_pitch, first, last, st, saved, false, input_ptr);
             const int done = (m == m_hi) ? last : std::min(last, m - r);
             for (int n = finished + 1; n <= done; ++n)
                 launch_normalize(n, out_ptr(n), out_pitch, st, saved);
@@ -653,11 +664,31 @@ int vsfeel_bm3d_trace_read(vsfeel_bm3d* ctx, double ms[VSFEEL_KERNEL_KINDS],
     });
 }
 
-int vsfeel_bm3d_process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
-                               int64_t src_row_stride, float* dst, int64_t dst_frame_stride,
-                               int64_t dst_row_stride, int first, int count, void* stream) {
+}  // extern "C"
+
+namespace {
+
+// The pass a call asks for must be the context's: a context created with a
+// "ref" clip runs the final pass and needs the ref frames, the others must
+// not get any.
+int check_pass(const vsfeel_bm3d* ctx, bool with_ref) {
+    if (ctx->s.final_pass && !with_ref)
+        return fail(VSFEEL_E_ARG,
+                    "the context runs the final pass: give the \"ref\" frames (the *_ref entry "
+                    "points)");
+    if (!ctx->s.final_pass && with_ref)
+        return fail(VSFEEL_E_ARG, "no \"ref\" clip was given when the context was created");
+    return VSFEEL_OK;
+}
+
+int process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
+                   int64_t src_row_stride, const float* ref, int64_t ref_frame_stride,
+                   int64_t ref_row_stride, float* dst, int64_t dst_frame_stride,
+                   int64_t dst_row_stride, int first, int count, void* stream) {
     return guarded(ctx, [&]() -> int {
         const Settings& s = ctx->s;
+        int rc = check_pass(ctx, ref != nullptr);
+        if (rc != VSFEEL_OK) return rc;
         if (!src || !dst) return fail(VSFEEL_E_ARG, "null frame buffer");
         if (first < 0 || count < 0 || first + count > s.nframes)
             return fail(VSFEEL_E_ARG, "output range outside the clip");
@@ -666,12 +697,183 @@ int vsfeel_bm3d_process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_f
             return fail(VSFEEL_E_ARG, "row stride smaller than the width");
         if (src_frame_stride < src_row_stride * s.height || dst_frame_stride < dst_row_stride * s.height)
             return fail(VSFEEL_E_ARG, "frame stride smaller than a plane");
+        if (ref && ref_row_stride != src_row_stride)
+            return fail(VSFEEL_E_ARG, "\"ref\" and \"clip\" frames must share a row stride");
+        if (ref && ref_frame_stride < ref_row_stride * s.height)
+            return fail(VSFEEL_E_ARG, "frame stride smaller than a plane");
         cudaStream_t st = (cudaStream_t)stream;
-        ctx->run([&](int f) { return src + (size_t)f * src_frame_stride; }, (int)src_row_stride,
-                 [&](int n) { return dst + (size_t)(n - first) * dst_frame_stride; },
-                 (int)dst_row_stride, first, count, st);
+        auto src_at = [&](int f) -> const float* { return src + (size_t)f * src_frame_stride; };
+        auto out_at = [&](int n) { return dst + (size_t)(n - first) * dst_frame_stride; };
+        if (!ref) {
+            ctx->run(src_at, (int)src_row_stride, out_at, (int)dst_row_stride, first, count, st);
+        } else {
+            // the final pass searches the ref clip and denoises the source
+            const std::function<const float*(int)> input = src_at;
+            ctx->run([&](int f) -> const float* { return ref + (size_t)f * ref_frame_stride; },
+                     (int)src_row_stride, out_at, (int)dst_row_stride, first, count, st, nullptr,
+                     &input);
+        }
         return VSFEEL_OK;
     });
+}
+
+// Host clip(s) -> staged device frames -> outputs -> host. In the final pass
+// the staging buffer holds the source frames, then the ref frames.
+int process_host(vsfeel_bm3d* ctx, const float* src, ptrdiff_t src_frame_stride_bytes,
+                 ptrdiff_t src_row_stride_bytes, const float* ref, ptrdiff_t ref_frame_stride_bytes,
+                 ptrdiff_t ref_row_stride_bytes, float* dst, ptrdiff_t dst_frame_stride_bytes,
+                 ptrdiff_t dst_row_stride_bytes, int first, int count) {
+    return guarded(ctx, [&]() -> int {
+        const Settings& s = ctx->s;
+        int rc = check_pass(ctx, ref != nullptr);
+        if (rc != VSFEEL_OK) return rc;
+        if (!src || !dst) return fail(VSFEEL_E_ARG, "null frame buffer");
+        if (first < 0 || count < 0 || first + count > s.nframes)
+            return fail(VSFEEL_E_ARG, "output range outside the clip");
+        const size_t row_bytes = sizeof(float) * (size_t)s.width;
+        if (src_row_stride_bytes < (ptrdiff_t)row_bytes || dst_row_stride_bytes < (ptrdiff_t)row_bytes ||
+            (ref && ref_row_stride_bytes < (ptrdiff_t)row_bytes))
+            return fail(VSFEEL_E_ARG, "row stride smaller than the width");
+        if (count == 0) return VSFEEL_OK;
+        const int r = s.radius;
+        const int f_lo = ctx->clampf(first - 2 * r), f_hi = ctx->clampf(first + count - 1 + 2 * r);
+        const int nin = f_hi - f_lo + 1;
+        const size_t ff = ctx->frame_floats();
+        ctx->frame_slot.clear();
+        ctx->slot_frame.clear();
+        ctx->frames.ensure(ff * nin * (ref ? 2 : 1));
+        ctx->outbuf.ensure(ff * count);
+        cudaStream_t st = ctx->stream;
+        auto upload = [&](const float* clip, ptrdiff_t fs, ptrdiff_t rs, float* base) {
+            for (int f = f_lo; f <= f_hi; ++f)
+                VSF_CUDA(cudaMemcpy2DAsync(base + (size_t)(f - f_lo) * ff,
+                                           sizeof(float) * ctx->acc_pitch,
+                                           (const char*)clip + (ptrdiff_t)f * fs, rs, row_bytes,
+                                           s.height, cudaMemcpyHostToDevice, st));
+        };
+        float* src_base = ctx->frames.p;
+        float* ref_base = ctx->frames.p + (size_t)nin * ff;
+        upload(src, src_frame_stride_bytes, src_row_stride_bytes, src_base);
+        if (ref) upload(ref, ref_frame_stride_bytes, ref_row_stride_bytes, ref_base);
+        auto src_at = [&](int f) -> const float* { return src_base + (size_t)(f - f_lo) * ff; };
+        auto out_at = [&](int n) { return ctx->outbuf.p + (size_t)(n - first) * ff; };
+        if (!ref) {
+            ctx->run(src_at, ctx->acc_pitch, out_at, ctx->acc_pitch, first, count, st);
+        } else {
+            const std::function<const float*(int)> input = src_at;
+            ctx->run([&](int f) -> const float* { return ref_base + (size_t)(f - f_lo) * ff; },
+                     ctx->acc_pitch, out_at, ctx->acc_pitch, first, count, st, nullptr, &input);
+        }
+        for (int q = 0; q < count; ++q)
+            VSF_CUDA(cudaMemcpy2DAsync((char*)dst + (ptrdiff_t)q * dst_frame_stride_bytes,
+                                       dst_row_stride_bytes, ctx->outbuf.p + (size_t)q * ff,
+                                       sizeof(float) * ctx->acc_pitch, row_bytes, s.height,
+                                       cudaMemcpyDeviceToHost, st));
+        return ctx->finish(st);
+    });
+}
+
+// The per-frame request path. fetch(clip, f, &stride) returns frame f of
+// the source (clip 0) or the ref clip (1); release(clip, f) hands it back.
+// A cache slot holds a frame's source plane and, in the final pass, its ref
+// plane after it.
+int get_frame(vsfeel_bm3d* ctx, int n, bool with_ref,
+              const std::function<const float*(int, int, ptrdiff_t*)>& fetch,
+              const std::function<void(int, int)>& release, float* dst, ptrdiff_t dst_stride_bytes) {
+    return guarded(ctx, [&]() -> int {
+        const Settings& s = ctx->s;
+        int rc = check_pass(ctx, with_ref);
+        if (rc != VSFEEL_OK) return rc;
+        if (!dst) return fail(VSFEEL_E_ARG, "null callback or destination");
+        if (n < 0 || n >= s.nframes) return fail(VSFEEL_E_ARG, "frame index out of range");
+        const size_t row_bytes = sizeof(float) * (size_t)s.width;
+        if (dst_stride_bytes < (ptrdiff_t)row_bytes)
+            return fail(VSFEEL_E_ARG, "row stride smaller than the width");
+        const int r = s.radius;
+        const int planes = with_ref ? 2 : 1;
+        const int f_lo = ctx->clampf(n - 2 * r), f_hi = ctx->clampf(n + 2 * r);
+        const int cap = 4 * r + 2;  // window plus one frame of slack
+        const size_t ff = ctx->frame_floats();
+        if ((int)ctx->slot_frame.size() != cap) {
+            ctx->frame_slot.clear();
+            ctx->slot_frame.assign(cap, -1);
+        }
+        ctx->frames.ensure(ff * cap * planes);
+        ctx->outbuf.ensure(ff);
+        cudaStream_t st = ctx->stream;
+        // evict cached frames outside the window, then upload the missing ones
+        for (auto it = ctx->frame_slot.begin(); it != ctx->frame_slot.end();) {
+            if (it->first < f_lo || it->first > f_hi) {
+                ctx->slot_frame[it->second] = -1;
+                it = ctx->frame_slot.erase(it);
+            } else {
+                ++it;
+            }
+        }
+        for (int f = f_lo; f <= f_hi; ++f) {
+            if (ctx->frame_slot.count(f)) continue;
+            int slot = 0;
+            while (ctx->slot_frame[slot] != -1) ++slot;
+            for (int clip = 0; clip < planes; ++clip) {
+                ptrdiff_t stride = 0;
+                const float* p = fetch(clip, f, &stride);
+                if (!p)
+                    return fail(VSFEEL_E_FETCH, std::string("could not fetch ") +
+                                                    (clip ? "\"ref\" frame " : "source frame ") +
+                                                    std::to_string(f));
+                if (stride < (ptrdiff_t)row_bytes) {
+                    release(clip, f);
+                    return fail(VSFEEL_E_ARG, "source row stride smaller than the width");
+                }
+                VSF_CUDA(cudaMemcpy2DAsync(ctx->frames.p + ((size_t)slot * planes + clip) * ff,
+                                           sizeof(float) * ctx->acc_pitch, p, stride, row_bytes,
+                                           s.height, cudaMemcpyHostToDevice, st));
+                // the source frame must stay valid until the copy has run
+                const int wrc = wait_stream(st, timeout_ms());
+                release(clip, f);
+                if (wrc != VSFEEL_OK) return wrc;
+            }
+            ctx->slot_frame[slot] = f;
+            ctx->frame_slot[f] = slot;
+        }
+        auto plane_at = [&](int f, int clip) -> const float* {
+            return ctx->frames.p + ((size_t)ctx->frame_slot.at(f) * planes + clip) * ff;
+        };
+        auto out_at = [&](int) { return ctx->outbuf.p; };
+        if (!with_ref) {
+            ctx->run([&](int f) { return plane_at(f, 0); }, ctx->acc_pitch, out_at, ctx->acc_pitch,
+                     n, 1, st);
+        } else {
+            const std::function<const float*(int)> input = [&](int f) { return plane_at(f, 0); };
+            ctx->run([&](int f) { return plane_at(f, 1); }, ctx->acc_pitch, out_at, ctx->acc_pitch,
+                     n, 1, st, nullptr, &input);
+        }
+        VSF_CUDA(cudaMemcpy2DAsync(dst, dst_stride_bytes, ctx->outbuf.p, sizeof(float) * ctx->acc_pitch,
+                                   row_bytes, s.height, cudaMemcpyDeviceToHost, st));
+        return ctx->finish(st);
+    });
+}
+
+}  // namespace
+
+extern "C" {
+
+int vsfeel_bm3d_process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
+                               int64_t src_row_stride, float* dst, int64_t dst_frame_stride,
+                               int64_t dst_row_stride, int first, int count, void* stream) {
+    return process_device(ctx, src, src_frame_stride, src_row_stride, nullptr, 0, 0, dst,
+                          dst_frame_stride, dst_row_stride, first, count, stream);
+}
+
+int vsfeel_bm3d_process_device_ref(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
+                                   int64_t src_row_stride, const float* ref,
+                                   int64_t ref_frame_stride, int64_t ref_row_stride, float* dst,
+                                   int64_t dst_frame_stride, int64_t dst_row_stride, int first,
+                                   int count, void* stream) {
+    if (!ref) return fail(VSFEEL_E_ARG, "null \"ref\" buffer");
+    return process_device(ctx, src, src_frame_stride, src_row_stride, ref, ref_frame_stride,
+                          ref_row_stride, dst, dst_frame_stride, dst_row_stride, first, count,
+                          stream);
 }
 
 int vsfeel_bm3d_saved_layout(const vsfeel_bm3d* ctx, vsfeel_bm3d_saved_info* out) {
@@ -694,6 +896,9 @@ int vsfeel_bm3d_forward_saved(vsfeel_bm3d* ctx, const float* src, int64_t src_fr
                               int64_t dst_row_stride, void* saved, void* stream) {
     return guarded(ctx, [&]() -> int {
         const Settings& s = ctx->s;
+        if (s.final_pass)
+            return fail(VSFEEL_E_UNSUPPORTED,
+                        "the differentiable form covers the basic estimate, not the final pass");
         if (!src || !dst || !saved) return fail(VSFEEL_E_ARG, "null buffer");
         if ((reinterpret_cast<uintptr_t>(saved) & 255u) != 0)
             return fail(VSFEEL_E_ARG, "saved-state buffer must be 256-byte aligned");
@@ -715,6 +920,9 @@ int vsfeel_bm3d_backward(vsfeel_bm3d* ctx, const void* saved, const float* grad_
                          int64_t gi_frame_stride, int64_t gi_row_stride, void* stream) {
     return guarded(ctx, [&]() -> int {
         const Settings& s = ctx->s;
+        if (s.final_pass)
+            return fail(VSFEEL_E_UNSUPPORTED,
+                        "the differentiable form covers the basic estimate, not the final pass");
         if (!saved || !grad_out || !grad_in) return fail(VSFEEL_E_ARG, "null buffer");
         if ((reinterpret_cast<uintptr_t>(saved) & 255u) != 0)
             return fail(VSFEEL_E_ARG, "saved-state buffer must be 256-byte aligned");
@@ -767,98 +975,44 @@ int vsfeel_bm3d_process_host(vsfeel_bm3d* ctx, const float* src, ptrdiff_t src_f
                              ptrdiff_t src_row_stride_bytes, float* dst,
                              ptrdiff_t dst_frame_stride_bytes, ptrdiff_t dst_row_stride_bytes,
                              int first, int count) {
-    return guarded(ctx, [&]() -> int {
-        const Settings& s = ctx->s;
-        if (!src || !dst) return fail(VSFEEL_E_ARG, "null frame buffer");
-        if (first < 0 || count < 0 || first + count > s.nframes)
-            return fail(VSFEEL_E_ARG, "output range outside the clip");
-        const size_t row_bytes = sizeof(float) * (size_t)s.width;
-        if (src_row_stride_bytes < (ptrdiff_t)row_bytes || dst_row_stride_bytes < (ptrdiff_t)row_bytes)
-            return fail(VSFEEL_E_ARG, "row stride smaller than the width");
-        if (count == 0) return VSFEEL_OK;
-        const int r = s.radius;
-        const int f_lo = ctx->clampf(first - 2 * r), f_hi = ctx->clampf(first + count - 1 + 2 * r);
-        const int nin = f_hi - f_lo + 1;
-        const size_t ff = ctx->frame_floats();
-        ctx->frame_slot.clear();
-        ctx->slot_frame.clear();
-        ctx->frames.ensure(ff * nin);
-        ctx->outbuf.ensure(ff * count);
-        cudaStream_t st = ctx->stream;
-        for (int f = f_lo; f <= f_hi; ++f)
-            VSF_CUDA(cudaMemcpy2DAsync(ctx->frames.p + (size_t)(f - f_lo) * ff,
-                                       sizeof(float) * ctx->acc_pitch,
-                                       (const char*)src + (ptrdiff_t)f * src_frame_stride_bytes,
-                                       src_row_stride_bytes, row_bytes, s.height,
-                                       cudaMemcpyHostToDevice, st));
-        ctx->run([&](int f) { return ctx->frames.p + (size_t)(f - f_lo) * ff; }, ctx->acc_pitch,
-                 [&](int n) { return ctx->outbuf.p + (size_t)(n - first) * ff; }, ctx->acc_pitch,
-                 first, count, st);
-        for (int q = 0; q < count; ++q)
-            VSF_CUDA(cudaMemcpy2DAsync((char*)dst + (ptrdiff_t)q * dst_frame_stride_bytes,
-                                       dst_row_stride_bytes, ctx->outbuf.p + (size_t)q * ff,
-                                       sizeof(float) * ctx->acc_pitch, row_bytes, s.height,
-                                       cudaMemcpyDeviceToHost, st));
-        return ctx->finish(st);
-    });
+    return process_host(ctx, src, src_frame_stride_bytes, src_row_stride_bytes, nullptr, 0, 0, dst,
+                        dst_frame_stride_bytes, dst_row_stride_bytes, first, count);
+}
+
+int vsfeel_bm3d_process_host_ref(vsfeel_bm3d* ctx, const float* src,
+                                 ptrdiff_t src_frame_stride_bytes, ptrdiff_t src_row_stride_bytes,
+                                 const float* ref, ptrdiff_t ref_frame_stride_bytes,
+                                 ptrdiff_t ref_row_stride_bytes, float* dst,
+                                 ptrdiff_t dst_frame_stride_bytes, ptrdiff_t dst_row_stride_bytes,
+                                 int first, int count) {
+    if (!ref) return fail(VSFEEL_E_ARG, "null \"ref\" buffer");
+    return process_host(ctx, src, src_frame_stride_bytes, src_row_stride_bytes, ref,
+                        ref_frame_stride_bytes, ref_row_stride_bytes, dst, dst_frame_stride_bytes,
+                        dst_row_stride_bytes, first, count);
 }
 
 int vsfeel_bm3d_get_frame(vsfeel_bm3d* ctx, int n, vsfeel_fetch_fn fetch, vsfeel_release_fn release,
                           void* user, float* dst, ptrdiff_t dst_stride_bytes) {
-    return guarded(ctx, [&]() -> int {
-        const Settings& s = ctx->s;
-        if (!fetch || !dst) return fail(VSFEEL_E_ARG, "null callback or destination");
-        if (n < 0 || n >= s.nframes) return fail(VSFEEL_E_ARG, "frame index out of range");
-        const size_t row_bytes = sizeof(float) * (size_t)s.width;
-        if (dst_stride_bytes < (ptrdiff_t)row_bytes)
-            return fail(VSFEEL_E_ARG, "row stride smaller than the width");
-        const int r = s.radius;
-        const int f_lo = ctx->clampf(n - 2 * r), f_hi = ctx->clampf(n + 2 * r);
-        const int cap = 4 * r + 2;  // window plus one frame of slack
-        const size_t ff = ctx->frame_floats();
-        if ((int)ctx->slot_frame.size() != cap) {
-            ctx->frame_slot.clear();
-            ctx->slot_frame.assign(cap, -1);
-        }
-        ctx->frames.ensure(ff * cap);
-        ctx->outbuf.ensure(ff);
-        cudaStream_t st = ctx->stream;
-        // evict cached frames outside the window, then upload the missing ones
-        for (auto it = ctx->frame_slot.begin(); it != ctx->frame_slot.end();) {
-            if (it->first < f_lo || it->first > f_hi) {
-                ctx->slot_frame[it->second] = -1;
-                it = ctx->frame_slot.erase(it);
-            } else {
-                ++it;
-            }
-        }
-        for (int f = f_lo; f <= f_hi; ++f) {
-            if (ctx->frame_slot.count(f)) continue;
-            int slot = 0;
-            while (ctx->slot_frame[slot] != -1) ++slot;
-            ptrdiff_t stride = 0;
-            const float* p = fetch(user, f, &stride);
-            if (!p) return fail(VSFEEL_E_FETCH, "could not fetch source frame " + std::to_string(f));
-            if (stride < (ptrdiff_t)row_bytes) {
-                if (release) release(user, f);
-                return fail(VSFEEL_E_ARG, "source row stride smaller than the width");
-            }
-            VSF_CUDA(cudaMemcpy2DAsync(ctx->frames.p + (size_t)slot * ff,
-                                       sizeof(float) * ctx->acc_pitch, p, stride, row_bytes,
-                                       s.height, cudaMemcpyHostToDevice, st));
-            // the source frame must stay valid until the copy has run
-            const int wrc = wait_stream(st, timeout_ms());
+    if (!fetch) return fail(VSFEEL_E_ARG, "null callback or destination");
+    return get_frame(
+        ctx, n, false, [&](int, int f, ptrdiff_t* stride) { return fetch(user, f, stride); },
+        [&](int, int f) {
             if (release) release(user, f);
-            if (wrc != VSFEEL_OK) return wrc;
-            ctx->slot_frame[slot] = f;
-            ctx->frame_slot[f] = slot;
-        }
-        ctx->run([&](int f) { return ctx->frames.p + (size_t)ctx->frame_slot.at(f) * ff; },
-                 ctx->acc_pitch, [&](int) { return ctx->outbuf.p; }, ctx->acc_pitch, n, 1, st);
-        VSF_CUDA(cudaMemcpy2DAsync(dst, dst_stride_bytes, ctx->outbuf.p, sizeof(float) * ctx->acc_pitch,
-                                   row_bytes, s.height, cudaMemcpyDeviceToHost, st));
-        return ctx->finish(st);
-    });
+        },
+        dst, dst_stride_bytes);
+}
+
+int vsfeel_bm3d_get_frame_ref(vsfeel_bm3d* ctx, int n, vsfeel_fetch2_fn fetch,
+                              vsfeel_release2_fn release, void* user, float* dst,
+                              ptrdiff_t dst_stride_bytes) {
+    if (!fetch) return fail(VSFEEL_E_ARG, "null callback or destination");
+    return get_frame(
+        ctx, n, true,
+        [&](int clip, int f, ptrdiff_t* stride) { return fetch(user, clip, f, stride); },
+        [&](int clip, int f) {
+            if (release) release(user, clip, f);
+        },
+        dst, dst_stride_bytes);
 }
 
 int vsfeel_bm3d_match_table_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,

@@ -57,56 +57,108 @@ __device__ __forceinline__ void transform_group_axis(float d[64], bool inverse) 
     }
 }
 
+// The 3D transform of a group held as d[k*8 + j] (patch k, row j; lane = column).
+__device__ __forceinline__ void forward3(float d[64], float* buf, int sub) {
+    transform_rows(d, false);
+    transpose_group(d, buf, sub);
+    transform_rows(d, false);
+    transpose_group(d, buf, sub);
+    transform_group_axis(d, false);
+}
+
+__device__ __forceinline__ void inverse3(float d[64], float* buf, int sub) {
+    transform_rows(d, true);
+    transpose_group(d, buf, sub);
+    transform_rows(d, true);
+    transpose_group(d, buf, sub);
+    transform_group_axis(d, true);
+}
+
+__device__ __forceinline__ void gather_group(float d[64], const float* const frames[kMaxTW],
+                                             int pitch, const uint32_t mxy[8], uint32_t zp,
+                                             int sub) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int z = (int)((zp >> (4 * k)) & 15u);
+        const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
+        const float* p = frames[z] + (size_t)my * pitch + mx + sub;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) d[k * 8 + j] = __ldg(p + (size_t)j * pitch);
+    }
+}
+
+// Collaborative Wiener filtering of the final pass (src/bm3d.comp:401-443):
+// d holds the transformed group of the clip denoised, r the transformed group
+// of the basic estimate at the same positions. Per coefficient
+// c = rr / (rr + SS) with rr = r*r and SS = SIGMA_Y*SIGMA_Y rounded products
+// and an unfused sum (a shader compiler folds the specialisation constant's
+// square), c = 1 at DC; d becomes d*c/4096. The squared coefficients are
+// summed as the reference does: per lane four partial sums by index mod 4
+// (ks += c*c fused), (ks0 + ks1) + (ks2 + ks3), then the pairwise tree over
+// the group's lanes in lane order. Returns the weight 1 / sum.
+__device__ __forceinline__ float wiener_coefficients(float d[64], const float r[64], float sy,
+                                                     int sub) {
+    const float ss = __fmul_rn(sy, sy);
+    float ks[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int i = 0; i < 64; ++i) {
+        const float rr = __fmul_rn(r[i], r[i]);
+        float c = __fdiv_rn(rr, __fadd_rn(rr, ss));
+        if (i == 0 && sub == 0) c = 1.0f;
+        const float val = __fmul_rn(d[i], c);
+        ks[i % 4] = __fmaf_rn(c, c, ks[i % 4]);
+        d[i] = __fmul_rn(val, 1.0f / 4096.0f);
+    }
+    const float mine = __fadd_rn(__fadd_rn(ks[0], ks[1]), __fadd_rn(ks[2], ks[3]));
+    const int base = (threadIdx.x & 31) & ~7;
+    float k[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) k[l] = __shfl_sync(0xffffffffu, mine, base + l);
+    const float sum = __fadd_rn(__fadd_rn(__fadd_rn(k[0], k[1]), __fadd_rn(k[2], k[3])),
+                                __fadd_rn(__fadd_rn(k[4], k[5]), __fadd_rn(k[6], k[7])));
+    return __fdiv_rn(1.0f, sum);
+}
+
 // Filters block b's group (matches mxy = x | y << 16, zp = 8 x 4-bit slice)
 // and scatters it into the stack's slices. kSaveMask also records the keep
 // bits, lane `sub` writing word mask_out[b * 8 + sub] (bit 8 * group
 // frequency + vertical frequency, of horizontal frequency sub). An invalid
 // group (valid == false) computes but writes nothing. buf: kGroupStride
 // floats of shared memory owned by the group.
-template <bool kSaveMask>
+template <bool kSaveMask, bool kWiener = false>
 __device__ __forceinline__ void filter_group(const StackJob& job, int b, bool valid,
                                              const uint32_t mxy[8], uint32_t zp, int sub,
                                              float* buf) {
-    const int pitch = job.pitch;
     float d[64];
+    float w;
+    if (kWiener) {
+        float r[64];
+        gather_group(r, job.slice_frame, job.pitch, mxy, zp, sub);
+        forward3(r, buf, sub);
+        gather_group(d, job.slice_input, job.pitch, mxy, zp, sub);
+        forward3(d, buf, sub);
+        w = wiener_coefficients(d, r, job.thr, sub);
+    } else {
+        gather_group(d, job.slice_frame, job.pitch, mxy, zp, sub);
+        forward3(d, buf, sub);
+        const float thr = job.thr;
+        int kept = 0;
+        uint64_t bits = 0;
 #pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int z = (int)((zp >> (4 * k)) & 15u);
-        const float* __restrict__ f = job.slice_frame[z];
-        const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
-        const float* p = f + (size_t)my * pitch + mx + sub;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) d[k * 8 + j] = __ldg(p + (size_t)j * pitch);
+        for (int i = 0; i < 64; ++i) {
+            const float t = (i == 0 && sub == 0) ? 0.0f : thr;
+            const bool keep = fabsf(d[i]) >= t;
+            kept += keep ? 1 : 0;
+            if (kSaveMask) bits |= keep ? (uint64_t(1) << i) : uint64_t(0);
+            d[i] = keep ? __fmul_rn(d[i], 1.0f / 4096.0f) : 0.0f;
+        }
+        if (kSaveMask && valid) job.mask_out[(size_t)b * 8 + sub] = bits;
+        kept += __shfl_xor_sync(0xffffffffu, kept, 1);
+        kept += __shfl_xor_sync(0xffffffffu, kept, 2);
+        kept += __shfl_xor_sync(0xffffffffu, kept, 4);
+        w = __fdiv_rn(1.0f, (float)kept);
     }
-
-    transform_rows(d, false);
-    transpose_group(d, buf, sub);
-    transform_rows(d, false);
-    transpose_group(d, buf, sub);
-    transform_group_axis(d, false);
-
-    const float thr = job.thr;
-    int kept = 0;
-    uint64_t bits = 0;
-#pragma unroll
-    for (int i = 0; i < 64; ++i) {
-        const float t = (i == 0 && sub == 0) ? 0.0f : thr;
-        const bool keep = fabsf(d[i]) >= t;
-        kept += keep ? 1 : 0;
-        if (kSaveMask) bits |= keep ? (uint64_t(1) << i) : uint64_t(0);
-        d[i] = keep ? __fmul_rn(d[i], 1.0f / 4096.0f) : 0.0f;
-    }
-    if (kSaveMask && valid) job.mask_out[(size_t)b * 8 + sub] = bits;
-    kept += __shfl_xor_sync(0xffffffffu, kept, 1);
-    kept += __shfl_xor_sync(0xffffffffu, kept, 2);
-    kept += __shfl_xor_sync(0xffffffffu, kept, 4);
-    const float w = __fdiv_rn(1.0f, (float)kept);
-
-    transform_rows(d, true);
-    transpose_group(d, buf, sub);
-    transform_rows(d, true);
-    transpose_group(d, buf, sub);
-    transform_group_axis(d, true);
+    inverse3(d, buf, sub);
 
     if (!valid) return;
     const float E = job.extractor;

@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(128) bm3d_match_kernel(const StackJob job) {
 
 // The standalone filter: 16 groups of 8 lanes per CTA, matches read from
 // the stack's match table.
-template <bool kSaveMask>
+template <bool kSaveMask, bool kWiener>
 __global__ void __launch_bounds__(128) bm3d_filter_kernel(const StackJob job) {
     __shared__ float smem[kFilterGroupsPerCta * kGroupStride];
     const int sub = threadIdx.x & 7;
@@ -275,7 +275,7 @@ __global__ void __launch_bounds__(128) bm3d_filter_kernel(const StackJob job) {
     const uint4 m0 = reinterpret_cast<const uint4*>(job.match_xy + (size_t)b * 8)[0];
     const uint4 m1 = reinterpret_cast<const uint4*>(job.match_xy + (size_t)b * 8)[1];
     const uint32_t mxy[8] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w};
-    filter_group<kSaveMask>(job, b, valid, mxy, job.match_z[b], sub, buf);
+    filter_group<kSaveMask, kWiener>(job, b, valid, mxy, job.match_z[b], sub, buf);
 }
 
 // ---------------------------------------------------------------------------
@@ -454,10 +454,12 @@ cudaError_t launch_match(const StackJob& job, cudaStream_t stream) {
 }
 
 cudaError_t launch_filter(const StackJob& job, cudaStream_t stream) {
-    if (job.mask_out)
-        bm3d_filter_kernel<true><<<block_grid(job), kThreads, 0, stream>>>(job);
+    if (job.wiener)
+        bm3d_filter_kernel<false, true><<<block_grid(job), kThreads, 0, stream>>>(job);
+    else if (job.mask_out)
+        bm3d_filter_kernel<true, false><<<block_grid(job), kThreads, 0, stream>>>(job);
     else
-        bm3d_filter_kernel<false><<<block_grid(job), kThreads, 0, stream>>>(job);
+        bm3d_filter_kernel<false, false><<<block_grid(job), kThreads, 0, stream>>>(job);
     return cudaGetLastError();
 }
 

@@ -93,6 +93,9 @@ int vsfeel_bm3d_process_device_noalloc(const vsfeel_bm3d_args* args,
     vsfeel_bm3d_info inf;
     int rc = parse_to_info(args, vi, &inf);
     if (rc != VSFEEL_OK) return rc;
+    if (args->has_ref)
+        return set_error(VSFEEL_E_UNSUPPORTED,
+                         "the allocation-free entry point runs the basic estimate only");
     const int W = inf.width, H = inf.height, N = inf.num_frames, r = inf.radius;
     if (!src || !dst) return set_error(VSFEEL_E_ARG, "null frame buffer");
     if (first < 0 || count < 0 || first + count > N)

@@ -169,11 +169,18 @@ class BM3DNode(VideoNode):
     """The filter's output clip. Frames are denoised on demand (``get_frame``,
     the VapourSynth request path) or all at once (``output``)."""
 
-    def __init__(self, clip: VideoNode, ctx: _Context):
+    def __init__(self, clip: VideoNode, ctx: _Context, ref: VideoNode | None = None):
         super().__init__([clip.plane_array(p) for p in range(clip.format.num_planes)], clip.format)
         self._src = clip
         self._ctx = ctx
         self._luma_src = np.ascontiguousarray(clip.plane_array(0), dtype=np.float32)
+        # the final (Wiener) pass: the basic estimate that matching runs on
+        self._luma_ref = (None if ref is None
+                          else np.ascontiguousarray(ref.plane_array(0), dtype=np.float32))
+
+    @property
+    def final_pass(self) -> bool:
+        return self._luma_ref is not None
 
     @property
     def info(self) -> _lib.Info:
@@ -190,37 +197,59 @@ class BM3DNode(VideoNode):
             raise Error("frame index out of range")
         src = self._luma_src
         out = np.empty((self.height, self.width), dtype=np.float32)
+        if self.final_pass:
+            clips = (src, self._luma_ref)
 
-        @_lib.FETCH_FN
-        def fetch(user, f, stride):
-            stride[0] = src.strides[1]
-            return src[f].ctypes.data
+            @_lib.FETCH2_FN
+            def fetch2(user, clip, f, stride):
+                stride[0] = clips[clip].strides[1]
+                return clips[clip][f].ctypes.data
 
-        @_lib.RELEASE_FN
-        def release(user, f):
-            pass
+            @_lib.RELEASE2_FN
+            def release2(user, clip, f):
+                pass
 
-        self._ctx.check(self._ctx.lib.vsfeel_bm3d_get_frame(
-            self._ctx.handle, n, fetch, release, None, out.ctypes.data, out.strides[0]))
+            self._ctx.check(self._ctx.lib.vsfeel_bm3d_get_frame_ref(
+                self._ctx.handle, n, fetch2, release2, None, out.ctypes.data, out.strides[0]))
+        else:
+            @_lib.FETCH_FN
+            def fetch(user, f, stride):
+                stride[0] = src.strides[1]
+                return src[f].ctypes.data
+
+            @_lib.RELEASE_FN
+            def release(user, f):
+                pass
+
+            self._ctx.check(self._ctx.lib.vsfeel_bm3d_get_frame(
+                self._ctx.handle, n, fetch, release, None, out.ctypes.data, out.strides[0]))
         planes = [out] + [self._src.plane_array(p)[n] for p in range(1, self.format.num_planes)]
         return VideoFrame(planes, self.format)
 
-    def output_device(self, src, out, first: int = 0, count: int | None = None) -> None:
+    def output_device(self, src, out, first: int = 0, count: int | None = None,
+                      ref=None) -> None:
         """Denoises from device memory: src is a CUDA float32 tensor
         (num_frames, H, W) holding the clip's luma, out receives frames
-        first..first+count-1 as (count, H, W). Enqueued on torch's current
-        stream; no host copies."""
+        first..first+count-1 as (count, H, W); in the final pass ref holds the
+        basic estimate's luma like src. Enqueued on torch's current stream;
+        no host copies."""
         import torch
 
         count = self.num_frames - first if count is None else count
-        for t in (src, out):
+        for t in (src, out) + ((ref,) if ref is not None else ()):
             if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32
                     and t.dim() == 3 and t.stride(2) == 1):
                 raise Error("BM3D: device buffers must be CUDA float32 (N, H, W) tensors")
         stream = torch.cuda.current_stream(src.device).cuda_stream
-        self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_device(
-            self._ctx.handle, src.data_ptr(), src.stride(0), src.stride(1), out.data_ptr(),
-            out.stride(0), out.stride(1), first, count, stream))
+        if ref is None:
+            self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_device(
+                self._ctx.handle, src.data_ptr(), src.stride(0), src.stride(1), out.data_ptr(),
+                out.stride(0), out.stride(1), first, count, stream))
+        else:
+            self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_device_ref(
+                self._ctx.handle, src.data_ptr(), src.stride(0), src.stride(1), ref.data_ptr(),
+                ref.stride(0), ref.stride(1), out.data_ptr(), out.stride(0), out.stride(1), first,
+                count, stream))
 
     def launch_count(self) -> int:
         return int(self._ctx.lib.vsfeel_bm3d_launch_count(self._ctx.handle))
@@ -243,23 +272,33 @@ class BM3DNode(VideoNode):
         if out is None:
             out = np.empty((count, self.height, self.width), dtype=np.float32)
         src = self._luma_src
-        self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_host(
-            self._ctx.handle, src.ctypes.data, src.strides[0], src.strides[1], out.ctypes.data,
-            out.strides[0], out.strides[1], first, count))
+        if self.final_pass:
+            ref = self._luma_ref
+            self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_host_ref(
+                self._ctx.handle, src.ctypes.data, src.strides[0], src.strides[1], ref.ctypes.data,
+                ref.strides[0], ref.strides[1], out.ctypes.data, out.strides[0], out.strides[1],
+                first, count))
+        else:
+            self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_host(
+                self._ctx.handle, src.ctypes.data, src.strides[0], src.strides[1],
+                out.ctypes.data, out.strides[0], out.strides[1], first, count))
         return out
 
 
 def BM3Dv2(clip: VideoNode, ref: VideoNode | None = None, sigma=None, block_step=None,
            bm_range=None, radius=None, ps_num=None, ps_range=None, num_streams=None,
            extractor_exp=None, device: int = 0) -> BM3DNode:
-    """core.vsfeel.BM3Dv2: the BM3D basic estimate (hard thresholding)."""
+    """core.vsfeel.BM3Dv2: the BM3D basic estimate (hard thresholding), or
+    with ``ref`` (a basic estimate of the same clip) the final Wiener pass."""
     if not isinstance(clip, VideoNode):
         clip = clip_from_array(np.asarray(clip))
+    if ref is not None and not isinstance(ref, VideoNode):
+        ref = clip_from_array(np.asarray(ref))
     args, keep = _make_args(ref, sigma, block_step, bm_range, radius, ps_num, ps_range,
                             num_streams, extractor_exp)
     ctx = _Context(clip, args, device)
     del keep
-    return BM3DNode(clip, ctx)
+    return BM3DNode(clip, ctx, ref)
 
 
 def bm3d_device(frames, sigma=None, block_step=None, bm_range=None, radius=None, ps_num=None,

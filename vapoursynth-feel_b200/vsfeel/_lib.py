@@ -21,8 +21,11 @@ EXPORTS = (
     "vsfeel_bm3d_free",
     "vsfeel_bm3d_frame_range",
     "vsfeel_bm3d_get_frame",
+    "vsfeel_bm3d_get_frame_ref",
     "vsfeel_bm3d_process_host",
+    "vsfeel_bm3d_process_host_ref",
     "vsfeel_bm3d_process_device",
+    "vsfeel_bm3d_process_device_ref",
     "vsfeel_bm3d_get_info",
     "vsfeel_bm3d_match_table_device",
     "vsfeel_bm3d_launch_count",
@@ -142,6 +145,9 @@ class BatchClassInfo(ctypes.Structure):
 FETCH_FN = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                             ctypes.POINTER(ctypes.c_ssize_t))
 RELEASE_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int)
+FETCH2_FN = ctypes.CFUNCTYPE(ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                             ctypes.POINTER(ctypes.c_ssize_t))
+RELEASE2_FN = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_int, ctypes.c_int)
 
 _lib = None
 
@@ -171,6 +177,14 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.vsfeel_bm3d_get_frame.restype = c_int
     lib.vsfeel_bm3d_process_host.argtypes = [c_p, c_p, c_sz, c_sz, c_p, c_sz, c_sz, c_int, c_int]
     lib.vsfeel_bm3d_process_host.restype = c_int
+    lib.vsfeel_bm3d_process_host_ref.argtypes = [c_p, c_p, c_sz, c_sz, c_p, c_sz, c_sz, c_p, c_sz,
+                                                 c_sz, c_int, c_int]
+    lib.vsfeel_bm3d_process_host_ref.restype = c_int
+    lib.vsfeel_bm3d_process_device_ref.argtypes = [c_p, c_p, c_i64, c_i64, c_p, c_i64, c_i64, c_p,
+                                                   c_i64, c_i64, c_int, c_int, c_p]
+    lib.vsfeel_bm3d_process_device_ref.restype = c_int
+    lib.vsfeel_bm3d_get_frame_ref.argtypes = [c_p, c_int, FETCH2_FN, RELEASE2_FN, c_p, c_p, c_sz]
+    lib.vsfeel_bm3d_get_frame_ref.restype = c_int
     lib.vsfeel_bm3d_process_device.argtypes = [c_p, c_p, c_i64, c_i64, c_p, c_i64, c_i64, c_int,
                                                c_int, c_p]
     lib.vsfeel_bm3d_process_device.restype = c_int
