@@ -307,8 +307,10 @@ void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
     for (int ci : cls.clips) {
         const Clip& c = b->clips[ci];
         const StackJob probe = b->make_job(c, cls.acc.p, 0, true);
+        // the persistent kernel runs the sliding scan (radius < 3)
         for (int s = 0; s < kTileShapes; ++s)
-            fits[s] = fits[s] && tile_shape_fits(probe, TileShape(s), kTableOnly);
+            fits[s] = fits[s] && c.info.radius < 3 &&
+                      tile_shape_fits(probe, TileShape(s), kTableOnly);
         max_nblocks = std::max(max_nblocks, (size_t)c.info.blocks_x * c.info.blocks_y);
     }
     int shape = -1;

@@ -443,13 +443,12 @@ int block_grid(const StackJob& job) { return (job.nbx * job.nby * 8 + kThreads -
 }  // namespace
 
 cudaError_t launch_match(const StackJob& job, cudaStream_t stream) {
-    if (job.radius < 3) {
-        const int shape = default_tile_shape(job, kTableOnly);
-        if (shape >= 0) return launch_match_tiles(job, TileShape(shape), kTableOnly, stream);
+    const int shape = default_tile_shape(job, kTableOnly);
+    if (shape >= 0) return launch_match_tiles(job, TileShape(shape), kTableOnly, stream);
+    if (job.radius < 3)
         bm3d_match_kernel<true><<<block_grid(job), kThreads, 0, stream>>>(job);
-    } else {
+    else
         bm3d_match_kernel<false><<<block_grid(job), kThreads, 0, stream>>>(job);
-    }
     return cudaGetLastError();
 }
 

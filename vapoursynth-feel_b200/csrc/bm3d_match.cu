@@ -54,14 +54,15 @@ int tile_count(const StackJob& job, TileShape shape) {
 }
 
 // True when the tiled kernel handles this configuration with this shape:
-// radius < 3 (the sliding scan), its shared memory fits, and every temporal
+// the sliding scan (radius < 3) in any mode or the exact scan (radius >= 3)
+// writing the match table, its shared memory fits, and every temporal
 // window is centred on a real match. (A corner block's spatial window holds
 // (min(R, W-8)+1) * (min(R, H-8)+1) candidates; with fewer than ps_num of
 // them the reference seeds a temporal window at (0, 0), which can lie
 // outside the tile's staged region.) Otherwise the caller uses the
 // direct-read kernel.
 bool tile_shape_fits(const StackJob& job, TileShape shape, TileMode mode) {
-    if (job.radius >= 3) return false;
+    if (job.radius >= 3 && mode != kTableOnly) return false;  // exact scan: table mode only
     if (plan_bytes(job, shape, mode) > kSmemBudget) return false;
     if (job.radius > 0) {
         const int cw = std::min(job.bm_range, job.width - 8) + 1;

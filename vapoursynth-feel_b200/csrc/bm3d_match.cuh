@@ -226,6 +226,100 @@ __device__ __forceinline__ void scan_chunk(const Region& reg, const float* cur_s
     }
 }
 
+// Exact scan (radius >= 3, src/bm3d.comp:512-526): candidate cx (relative
+// to the window's left column) has the true 8x8 SSD
+//     E = ((S0 + S1) + (S2 + S3)) + ((S4 + S5) + (S6 + S7)),
+//     S_c = SSD(source column left + cx + c, block column c),
+// each column SSD in the reference's even/odd order. Step j loads source
+// column left + j and computes S_c for the 8 block columns; S_c belongs to
+// candidate j - c. Per row the tree advances incrementally on the
+// reference's operands: P01(j-1) = S0(j-1) + S1(j), P23(j-3) = S2(j-1) +
+// S3(j), P45(j-5) = S4(j-1) + S5(j), P67(j-7) = S6(j-1) + S7(j),
+// Q0123(j-3) = P01(j-3) + P23(j-3), Q4567(j-7) = P45(j-7) + P67(j-7),
+// E(j-7) = Q0123(j-7) + Q4567(j-7). Each block column is read from shared
+// memory once per step and used for all K rows. With 136 flops per candidate
+// the selection is cheap next to the scan, so there is no error table: each
+// candidate's (error, scan index) key goes straight into the lane's sorted
+// top-8 (top, ascending), and the 8 lane lists are merged afterwards.
+__device__ __forceinline__ void insert_key(uint64_t top[8], uint64_t key) {
+    if (key < top[7]) {
+#pragma unroll
+        for (int k = 7; k > 0; --k) {
+            const bool shift = key < top[k - 1];
+            top[k] = shift ? top[k - 1] : (key < top[k] ? key : top[k]);
+        }
+        top[0] = key < top[0] ? key : top[0];
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void scan_chunk_exact(const Region& reg, const float* cur_s,
+                                                 const Window& win, int r0, int nrows, int jcount,
+                                                 uint64_t top[8]) {
+    float s0p[K], s2p[K], s4p[K], s6p[K];  // S0, S2, S4, S6 of the previous step
+    float p01[K][2], p45[K][2], q0123[K][4];
+#pragma unroll
+    for (int q = 0; q < K; ++q) {
+        s0p[q] = s2p[q] = s4p[q] = s6p[q] = 0.0f;
+        p01[q][0] = p01[q][1] = p45[q][0] = p45[q][1] = 0.0f;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) q0123[q][i] = 0.0f;
+    }
+    const int xmax = win.left + win.rw + 6;
+    const float* sbase = reg.smem + (r0 - reg.ry0) - reg.rx0 * reg.cs;
+    const int cs = reg.cs;
+    const int seq0 = win.seq_base + (r0 - win.top) * win.rw;
+
+    for (int j0 = 0; j0 < jcount; j0 += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = j0 + u;
+            float w[K + 7];
+            {
+                const float* col = sbase + min(win.left + j, xmax) * cs;
+#pragma unroll
+                for (int k = 0; k < K + 7; ++k) w[k] = col[k];
+            }
+            float S[K][8];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                float b[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) b[i] = cur_s[c * 8 + i];
+#pragma unroll
+                for (int q = 0; q < K; ++q) S[q][c] = column_ssd_at<K>(b, w, q);
+            }
+            float e[K];
+#pragma unroll
+            for (int q = 0; q < K; ++q) {
+                const float np01 = __fadd_rn(s0p[q], S[q][1]);
+                const float np23 = __fadd_rn(s2p[q], S[q][3]);
+                const float np45 = __fadd_rn(s4p[q], S[q][5]);
+                const float np67 = __fadd_rn(s6p[q], S[q][7]);
+                // P01(j-3) and P45(j-7) were made two steps ago, Q0123(j-7) four
+                const float nq0123 = __fadd_rn(p01[q][u & 1], np23);
+                const float nq4567 = __fadd_rn(p45[q][u & 1], np67);
+                e[q] = __fadd_rn(q0123[q][u & 3], nq4567);
+                p01[q][u & 1] = np01;
+                p45[q][u & 1] = np45;
+                q0123[q][u & 3] = nq0123;
+                s0p[q] = S[q][0];
+                s2p[q] = S[q][2];
+                s4p[q] = S[q][4];
+                s6p[q] = S[q][6];
+            }
+            const int d = j - 7;
+            if (d >= 0 && d < win.rw && j < jcount) {
+#pragma unroll
+                for (int q = 0; q < K; ++q)
+                    // errors at or above FLT_MAX never count (src/bm3d.comp:284-302)
+                    if (q < nrows && e[q] < kFltMax)
+                        insert_key(top, make_key(e[q], seq0 + q * win.rw + d));
+            }
+        }
+    }
+}
+
 __device__ __forceinline__ int rows_per_lane(int total_rows) {
     return min(kMaxK, max(kMinK, (total_rows + 7) / 8));
 }
@@ -242,6 +336,32 @@ struct GroupState {
     uint64_t buf[kCollect];
     int count;
 };
+
+// The 8 smallest keys of the group's 8 sorted lane lists, into gs->top.
+__device__ __forceinline__ void merge_top8(uint64_t top[8], GroupState* gs, unsigned gmask) {
+    const int sub = threadIdx.x & 7;
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+        uint64_t best = top[0];
+        int src = sub;
+#pragma unroll
+        for (int off = 1; off < 8; off <<= 1) {
+            const uint64_t o = __shfl_xor_sync(gmask, best, off);
+            const int os = __shfl_xor_sync(gmask, src, off);
+            const bool take = o < best || (o == best && os < src);
+            best = take ? o : best;
+            src = take ? os : src;
+        }
+        if (sub == 0) gs->top[r] = best;
+        if (sub == src) {
+#pragma unroll
+            for (int i = 0; i < 7; ++i) top[i] = top[i + 1];
+            top[7] = kKeyMax;
+        }
+    }
+    __syncwarp(gmask);
+}
+
 
 // The 8 smallest (error, scan index) keys of the windows' error table into
 // gs->top (padded with (FLT_MAX, INT_MAX) when fewer exist; errors >= FLT_MAX
@@ -354,19 +474,25 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
 // Scans windows[0..nwin) of this lane's block into its error table, then
 // selects the top-8 into gs->top. Rows are split into chunks of K
 // (warp-uniform); chunk c of the block goes to lane c % 8 in round c / 8.
+template <bool kExact>
 __device__ void search_windows(const Region& reg, const float* cur_s, const float c7[8],
                                const Window* wins, int nwin, float* E, GroupState* gs,
                                unsigned gmask, int* status) {
     const int sub = threadIdx.x & 7;
     int total_rows = 0;
     for (int i = 0; i < nwin; ++i) total_rows += wins[i].h;
-    const int K = warp_max(rows_per_lane(total_rows));
+    // the exact scan keeps 8 column sums per row: at most 3 rows per lane
+    const int K = warp_max(kExact ? min(3, rows_per_lane(total_rows)) : rows_per_lane(total_rows));
     int ntasks = 0;
     for (int i = 0; i < nwin; ++i) ntasks += (wins[i].h + K - 1) / K;
     const int rounds = warp_max((ntasks + 7) / 8);
     float lb[8];
+    uint64_t top[8];
 #pragma unroll
-    for (int i = 0; i < 8; ++i) lb[i] = kFltMax;
+    for (int i = 0; i < 8; ++i) {
+        lb[i] = kFltMax;
+        top[i] = kKeyMax;
+    }
     for (int round = 0; round < rounds; ++round) {
         const int task = round * 8 + sub;
         const bool has = task < ntasks;
@@ -389,15 +515,25 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
             nrows = 0;
         }
         const int jcount = warp_max(has ? win.rw + 7 : 8);
-        switch (K) {
-            case 2: scan_chunk<2>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
-            case 3: scan_chunk<3>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
-            case 4: scan_chunk<4>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
-            default: scan_chunk<5>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
+        if (kExact) {
+            switch (K) {
+                case 2: scan_chunk_exact<2>(reg, cur_s, win, r0, nrows, jcount, top); break;
+                default: scan_chunk_exact<3>(reg, cur_s, win, r0, nrows, jcount, top); break;
+            }
+        } else {
+            switch (K) {
+                case 2: scan_chunk<2>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
+                case 3: scan_chunk<3>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
+                case 4: scan_chunk<4>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
+                default: scan_chunk<5>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
+            }
         }
     }
     __syncwarp(gmask);
-    select_top8(E, wins, nwin, lb, gs, gmask);
+    if (kExact)
+        merge_top8(top, gs, gmask);
+    else
+        select_top8(E, wins, nwin, lb, gs, gmask);
 }
 
 // global list insertion of a temporal match (src/bm3d.comp:304-322)
@@ -467,7 +603,8 @@ __host__ __device__ inline SmemPlan smem_plan(const StackJob& job, int mode) {
     const int h = tile_h + 2 * reach < job.height ? tile_h + 2 * reach : job.height;
     const int cs = (h + kMaxK + 7) | 1;
     p.region_floats = cs * w;
-    p.estride = ((error_table_floats(job) + 31) & ~31) + 8;
+    // the exact scan (radius >= 3) selects without error tables
+    p.estride = job.radius >= 3 ? 0 : ((error_table_floats(job) + 31) & ~31) + 8;
     p.etab_floats = kGroups * p.estride;
     if (mode != kTableOnly && p.etab_floats < kGroups * kGroupStride)
         p.etab_floats = kGroups * kGroupStride;
@@ -480,7 +617,7 @@ __host__ __device__ inline SmemPlan smem_plan(const StackJob& job, int mode) {
 // filtering of their groups. Shared memory: block state, windows, reference
 // blocks, error tables (the fused filter's buffers afterwards), then the
 // staged region. Every thread of the CTA calls it.
-template <int TX, int TY, int kMode>
+template <int TX, int TY, int kMode, bool kExact = false>
 __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
                                            unsigned char* smem_raw) {
     constexpr int kGroups = TX * TY;
@@ -552,7 +689,7 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         const Region s = stage(fc, R);
         if (sub == 0) win[0] = make_window(x, y, R, W, H, 0, 0);
         __syncwarp(gmask);
-        search_windows(s, cur_s, c7, win, 1, E, gs, gmask, job.status);
+        search_windows<kExact>(s, cur_s, c7, win, 1, E, gs, gmask, job.status);
         const uint64_t k = gs->top[sub];
         const uint32_t xy = key_xy(k, win, 0);
         gs->ge[sub] = key_err(k);
@@ -579,7 +716,7 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
                 }
             }
             __syncwarp(gmask);
-            search_windows(s, cur_s, c7, win, P, E, gs, gmask, job.status);
+            search_windows<kExact>(s, cur_s, c7, win, P, E, gs, gmask, job.status);
             if (sub == 0) {
                 for (int i = 0; i < P; ++i) {
                     const uint64_t k = gs->top[i];
@@ -647,6 +784,13 @@ __global__ void __launch_bounds__(TX * TY * 8, 1) bm3d_match_sliding_kernel(cons
     match_tile<TX, TY, kMode>(job, blockIdx.x, smem_raw);
 }
 
+// radius >= 3: the same tile body with the exact scan (match table only)
+template <int TX, int TY>
+__global__ void __launch_bounds__(TX * TY * 8, 1) bm3d_match_exact_kernel(const StackJob job) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    match_tile<TX, TY, kTableOnly, true>(job, blockIdx.x, smem_raw);
+}
+
 // Persistent form: every CTA pulls (stack, tile) items from the queue.
 // Thread 0 claims the next item while the current one runs (the atomic's
 // latency hides behind the tile), and the item's StackJob is copied to
@@ -712,6 +856,16 @@ cudaError_t launch_grid(const StackJob& job, size_t smem, cudaStream_t stream) {
 template <int TX, int TY>
 cudaError_t launch_grid_mode(const StackJob& job, TileMode mode, cudaStream_t stream) {
     const size_t smem = smem_plan<TX, TY>(job, mode).bytes;
+    if (job.radius >= 3) {
+        if (mode != kTableOnly) return cudaErrorInvalidValue;
+        auto* fn = bm3d_match_exact_kernel<TX, TY>;
+        cudaError_t e =
+            cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        const int tiles = ((job.nbx + TX - 1) / TX) * ((job.nby + TY - 1) / TY);
+        fn<<<tiles, TX * TY * 8, smem, stream>>>(job);
+        return cudaGetLastError();
+    }
     switch (mode) {
         case kTableOnly: return launch_grid<TX, TY, kTableOnly>(job, smem, stream);
         case kFused: return launch_grid<TX, TY, kFused>(job, smem, stream);
