@@ -57,6 +57,7 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMinK = 2, kMaxK = 5;
 constexpr int kCollect = 64;                // candidates a block collects per pass
+constexpr int kLaneHits = 8;                // hits a lane holds in registers (first pass)
 constexpr uint64_t kKeyMax = (uint64_t(0x7f7fffffu) << 32) | 0x7fffffffu;  // (FLT_MAX, INT_MAX)
 
 __device__ __forceinline__ uint64_t make_key(float err, int seq) {
@@ -393,8 +394,87 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
         }
     }
     uint64_t tkey = (uint64_t(__float_as_uint(bound)) << 32) | 0xffffffffu;
-    int n;
-    for (;;) {
+    int n = 0;
+    // First pass: every lane keeps its hits (error at or below the bound) in
+    // registers as (error, window << 24 | table index) -- a few selects per
+    // hit instead of a division and a shared atomic -- then turns them into
+    // (error, scan index) keys in a loop all lanes run together and places
+    // them by a prefix sum over the group. A group with a lane of more than
+    // kLaneHits hits, or more than kCollect in all, takes the general loop
+    // below (rare).
+    bool fast = false;
+    {
+        const float terr = bound;
+        float he[kLaneHits];
+        uint32_t hf[kLaneHits];
+#pragma unroll
+        for (int i = 0; i < kLaneHits; ++i) {
+            he[i] = 0.0f;
+            hf[i] = 0u;
+        }
+        int nh = 0;
+        for (int wi = 0; wi < nwin; ++wi) {
+            const Window w = wins[wi];
+            const int n_w = w.rw * w.h;
+            const int nq = (n_w + 3) >> 2;
+            const float4* tab = reinterpret_cast<const float4*>(E + w.eoff);
+            for (int v0 = 0; v0 < nq; v0 += 32) {
+                float4 q[4];
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int v = v0 + sub + 8 * k;
+                    q[k] = v < nq ? tab[v] : make_float4(kFltMax, kFltMax, kFltMax, kFltMax);
+                }
+                float mn = kFltMax;
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    mn = fminf(mn, fminf(fminf(q[k].x, q[k].y), fminf(q[k].z, q[k].w)));
+                if (!(mn <= terr)) continue;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float ev[4] = {q[k].x, q[k].y, q[k].z, q[k].w};
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int f = 4 * (v0 + sub + 8 * k) + u;
+                        if (f < n_w && ev[u] <= terr && ev[u] < kFltMax) {
+#pragma unroll
+                            for (int i = 0; i < kLaneHits; ++i) {
+                                he[i] = i == nh ? ev[u] : he[i];
+                                hf[i] = i == nh ? (uint32_t(wi) << 24) | uint32_t(f) : hf[i];
+                            }
+                            ++nh;
+                        }
+                    }
+                }
+            }
+        }
+        const int cnt = min(nh, kLaneHits);
+        int incl = cnt;
+#pragma unroll
+        for (int off = 1; off < 8; off <<= 1) {
+            const int t = __shfl_up_sync(gmask, incl, off, 8);
+            if (sub >= off) incl += t;
+        }
+        const int total = __shfl_sync(gmask, incl, 7, 8);
+        const bool overflow = __any_sync(gmask, nh > kLaneHits) || total > kCollect;
+        if (!overflow) {
+            const int excl = incl - cnt;
+#pragma unroll
+            for (int i = 0; i < kLaneHits; ++i) {
+                if (i < cnt) {
+                    const Window w = wins[hf[i] >> 24];
+                    const int f = int(hf[i] & 0xffffffu);
+                    const int d = f / w.h;
+                    const int row = f - d * w.h;
+                    gs->buf[excl + i] = make_key(he[i], w.seq_base + row * w.rw + d);
+                }
+            }
+            n = total;
+            fast = true;
+        }
+        __syncwarp(gmask);
+    }
+    while (!fast) {
         if (sub == 0) gs->count = 0;
         __syncwarp(gmask);
         const float terr = key_err(tkey);
