@@ -239,10 +239,12 @@ VSFEEL_API int vsfeel_bm3d_backward(vsfeel_bm3d* ctx, const void* saved, const f
  * Many clips of uneven sizes and settings denoised together; this replaces
  * the reference's num_streams concurrency. Clips are grouped into shape
  * classes (equal radius, block_step, bm_range, ps_num and ps_range). Per
- * class, one persistent launch works through a device queue of
- * (stack, tile) items of all the class's clips, matching each tile, one
- * launch filters every block of every stack and one normalises all the
- * class's output frames; the class's work is captured once in a CUDA graph. Classes run concurrently. With
+ * class, the clips are cut into chunks of whole clips (at least ~16 waves
+ * of tiles); per chunk one persistent launch works through a device queue
+ * of (stack, tile) items of its clips, matching each tile, one launch
+ * filters every block of its stacks and one normalises its output frames.
+ * The class's work is captured once in a CUDA graph; a run replays the
+ * classes' graphs one after another on the caller's stream. With
  * VSFEEL_BATCH_AUTOTUNE, vsfeel_bm3d_batch_create times every tile shape
  * that fits a class on one of its stacks and keeps the fastest; otherwise
  * the largest fitting shape is used. A class that no shape fits (radius >= 3,

@@ -13,15 +13,18 @@
 //   * norm[]: one NormalizeJob per output frame, with the prefix sums of
 //     their 32x8 tiles;
 //   * a match table per stack;
-//   * a CUDA graph: clear the class's accumulators and queue counter, the
-//     persistent matching launch (one CTA per SM) over the queue, one filter
-//     launch over every block of every stack, one normalise launch. (The
+//   * a CUDA graph: per chunk, clear its accumulators, the persistent
+//     matching launch (one CTA per SM) over its queue, one filter launch over
+//     every block of its stacks, one normalise launch. (The
 //     filter stays a separate kernel: inside the matcher's one CTA per SM
 //     its atomics run slower than at the filter kernel's occupancy.)
 //     Classes whose stacks no tile shape fits record the direct-read match
 //     and filter kernels per stack instead.
-// A run forks the caller's stream into one stream per class, replays the
-// graphs and joins back.
+// Classes are cut into chunks of whole clips (at least ~16 waves of tiles
+// each), matched, filtered and normalised chunk after chunk, so a chunk's
+// frames and accumulators are still in L2 when its filter and normalisation
+// run. A run replays the class graphs one after another on the caller's
+// stream.
 #include "bm3d_device.cuh"
 #include "vsfeel_bm3d.h"
 
@@ -91,6 +94,25 @@ int wait_stream(cudaStream_t s) {
     }
 }
 
+// Bounded wait for an event (the end of the last run).
+int wait_event(cudaEvent_t ev) {
+    const auto t0 = std::chrono::steady_clock::now();
+    const int64_t limit = timeout_ms();
+    for (int spins = 0;; ++spins) {
+        const cudaError_t e = cudaEventQuery(ev);
+        if (e == cudaSuccess) return VSFEEL_OK;
+        if (e != cudaErrorNotReady)
+            return error(VSFEEL_E_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
+        const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                            std::chrono::steady_clock::now() - t0)
+                            .count();
+        if (ms >= limit)
+            return error(VSFEEL_E_TIMEOUT,
+                         "timed out after " + std::to_string(ms) + " ms waiting for the GPU");
+        if (spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
 template <class T>
 struct Dev {
     T* p = nullptr;
@@ -146,6 +168,14 @@ struct Class {
     Dev<int> d_filter_first;
     int filter_items = 0;
     Dev<int> counter;
+    // chunks of whole clips, each matched, filtered and normalised in turn
+    struct Chunk {
+        int job0, njobs, norm0, nnorm;     // ranges in jobs[] and norm[]
+        int first_off, ffirst_off, nfirst_off;  // chunk-relative prefix arrays
+        int tiles, filter_items, norm_tiles;
+        size_t acc0, acc_floats;           // accumulator range
+    };
+    std::vector<Chunk> chunks;
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
     cudaGraph_t graph = nullptr;
@@ -160,10 +190,11 @@ struct vsfeel_bm3d_batch {
     std::vector<Clip> clips;
     std::vector<Class> classes;
     Dev<int> status;
-    cudaEvent_t start = nullptr;
+    cudaEvent_t start = nullptr;  // recorded after each run's last graph
     int64_t device_bytes = 0;
 
     ~vsfeel_bm3d_batch() {
+        if (start) wait_event(start);
         for (Class& c : classes) {
             if (c.stream) wait_stream(c.stream);
             if (c.exec) cudaGraphExecDestroy(c.exec);
@@ -297,7 +328,6 @@ void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
         acc_floats += (c.acc_floats() + 63) & ~size_t(63);
     }
     cls.acc.alloc(acc_floats);
-    cls.counter.alloc(1);
     b->device_bytes += (int64_t)acc_floats * 4;
 
     // which tile shapes fit every stack of the class
@@ -333,18 +363,53 @@ void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
     cls.tile_shape = shape;
 
     // queue of (stack, tile) items and the normalisation list
-    std::vector<int> first{0}, nfirst{0}, ffirst{0};
+    // Jobs and outputs, and chunks of whole clips of at least kChunkTiles
+    // queue items (about 16 waves): a chunk's frames and accumulators are
+    // still in L2 when its filter and normalisation run, while the
+    // persistent launch keeps small clips together.
+    const int64_t kChunkTiles = (int64_t)b->sms * 16;
+    std::vector<int> first, nfirst, ffirst;  // chunk-relative prefix sums, chunk after chunk
     std::vector<NormalizeJob> norm;
+    Class::Chunk cur{};
+    auto open_chunk = [&](size_t acc0) {
+        cur = Class::Chunk{};
+        cur.job0 = (int)cls.jobs.size();
+        cur.norm0 = (int)norm.size();
+        cur.first_off = (int)first.size();
+        cur.ffirst_off = (int)ffirst.size();
+        cur.nfirst_off = (int)nfirst.size();
+        cur.acc0 = acc0;
+        first.push_back(0);
+        ffirst.push_back(0);
+        nfirst.push_back(0);
+    };
+    auto close_chunk = [&](size_t acc_end) {
+        cur.njobs = (int)cls.jobs.size() - cur.job0;
+        cur.nnorm = (int)norm.size() - cur.norm0;
+        cur.tiles = first.back();
+        cur.filter_items = ffirst.back();
+        cur.norm_tiles = nfirst.back();
+        cur.acc_floats = acc_end - cur.acc0;
+        cls.chunks.push_back(cur);
+    };
+    bool open = false;
+    size_t acc_end = 0;
     for (int ci : cls.clips) {
         const Clip& c = b->clips[ci];
         const int N = c.info.num_frames, r = c.info.radius, tw = c.tw();
+        if (!open) {
+            open_chunk(c.acc_off);
+            open = true;
+        }
         for (int m = 0; m < N; ++m) {
             StackJob job = b->make_job(c, cls.acc.p, m, false);
             if (shape >= 0) {
                 cls.smem = std::max(cls.smem, tile_smem_bytes(job, TileShape(shape), kTableOnly));
-                first.push_back(first.back() + tile_count(job, TileShape(shape)));
+                const int64_t t = (int64_t)first.back() + tile_count(job, TileShape(shape));
                 const int64_t fi = (int64_t)ffirst.back() + filter_items(c.info.blocks_x * c.info.blocks_y);
-                if (fi > INT32_MAX) throw Fail{VSFEEL_E_ARG, "batch too large for one filter launch"};
+                if (t > INT32_MAX || fi > INT32_MAX)
+                    throw Fail{VSFEEL_E_ARG, "batch too large for one launch"};
+                first.push_back((int)t);
                 ffirst.push_back((int)fi);
             }
             cls.jobs.push_back(job);
@@ -367,9 +432,14 @@ void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
             if (nt > INT32_MAX) throw Fail{VSFEEL_E_ARG, "batch too large for one normalise launch"};
             nfirst.push_back((int)nt);
         }
+        acc_end = c.acc_off + c.acc_floats();
+        if (shape < 0 || first.back() >= kChunkTiles) {
+            close_chunk(acc_end);
+            open = false;
+        }
     }
-    if (shape >= 0 && first.back() < 0) throw Fail{VSFEEL_E_ARG, "batch too large for one queue"};
-    cls.tiles = shape >= 0 ? first.back() : 0;
+    if (open) close_chunk(acc_end);
+    for (const Class::Chunk& ch : cls.chunks) cls.tiles += ch.tiles;
     if (shape < 0) {
         // direct-read kernels, stack after stack: one match table suffices
         cls.match_xy.alloc(max_nblocks * 8);
@@ -379,7 +449,7 @@ void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
             j.match_z = cls.match_z.p;
         }
     } else {
-        // every stack is in flight at once: one match table each
+        // every stack of a chunk is in flight at once: one match table each
         size_t total = 0;
         for (const StackJob& j : cls.jobs) total += (size_t)j.nbx * j.nby;
         cls.match_xy.alloc(total * 8);
@@ -391,37 +461,41 @@ void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
             off += (size_t)j.nbx * j.nby;
         }
         cls.d_filter_first.upload(ffirst);
-        cls.filter_items = ffirst.back();
+        cls.d_tile_first.upload(first);
     }
     cls.d_jobs.upload(cls.jobs);
-    if (shape >= 0) cls.d_tile_first.upload(first);
     cls.d_norm.upload(norm);
     cls.d_norm_first.upload(nfirst);
     cls.nnorm = (int)norm.size();
-    cls.norm_tiles = nfirst.back();
+    cls.counter.alloc(cls.chunks.size());
     b->device_bytes += (int64_t)(cls.match_xy.n + cls.match_z.n) * 4;
 
-    // capture the class's run
+    // capture the class's run: per chunk, clear its accumulators, match,
+    // filter, normalise
     check(cudaStreamBeginCapture(cls.stream, cudaStreamCaptureModeRelaxed), "capture");
-    cudaError_t err = cudaMemsetAsync(cls.acc.p, 0, acc_floats * sizeof(float), cls.stream);
-    if (err == cudaSuccess && shape >= 0) {
-        err = cudaMemsetAsync(cls.counter.p, 0, sizeof(int), cls.stream);
-        const BatchWork work{cls.d_jobs.p, cls.d_tile_first.p, (int)cls.jobs.size(), cls.counter.p};
-        const int grid = (int)std::min<int64_t>(b->sms, cls.tiles);
-        if (err == cudaSuccess)
+    cudaError_t err = cudaMemsetAsync(cls.counter.p, 0, sizeof(int) * cls.chunks.size(), cls.stream);
+    for (size_t k = 0; k < cls.chunks.size() && err == cudaSuccess; ++k) {
+        const Class::Chunk& ch = cls.chunks[k];
+        err = cudaMemsetAsync(cls.acc.p + ch.acc0, 0, ch.acc_floats * sizeof(float), cls.stream);
+        if (err == cudaSuccess && shape >= 0) {
+            const BatchWork work{cls.d_jobs.p + ch.job0, cls.d_tile_first.p + ch.first_off, ch.njobs,
+                                 cls.counter.p + k};
+            const int grid = std::min(b->sms, ch.tiles);
             err = launch_batch_tiles(work, TileShape(shape), kTableOnly, cls.smem, grid, cls.stream);
-        const FilterBatch fw{cls.d_jobs.p, cls.d_filter_first.p, (int)cls.jobs.size()};
-        if (err == cudaSuccess) err = launch_filter_batch(fw, cls.filter_items, cls.stream);
-    } else if (err == cudaSuccess) {
-        for (const StackJob& j : cls.jobs) {
-            err = launch_match(j, cls.stream);
-            if (err == cudaSuccess) err = launch_filter(j, cls.stream);
-            if (err != cudaSuccess) break;
+            const FilterBatch fw{cls.d_jobs.p + ch.job0, cls.d_filter_first.p + ch.ffirst_off,
+                                 ch.njobs};
+            if (err == cudaSuccess) err = launch_filter_batch(fw, ch.filter_items, cls.stream);
+        } else if (err == cudaSuccess) {
+            for (int j = ch.job0; j < ch.job0 + ch.njobs && err == cudaSuccess; ++j) {
+                err = launch_match(cls.jobs[j], cls.stream);
+                if (err == cudaSuccess) err = launch_filter(cls.jobs[j], cls.stream);
+            }
         }
-    }
-    if (err == cudaSuccess) {
-        const NormalizeBatch nw{cls.d_norm.p, cls.d_norm_first.p, cls.nnorm};
-        err = launch_normalize_batch(nw, cls.norm_tiles, cls.stream);
+        if (err == cudaSuccess) {
+            const NormalizeBatch nw{cls.d_norm.p + ch.norm0, cls.d_norm_first.p + ch.nfirst_off,
+                                    ch.nnorm};
+            err = launch_normalize_batch(nw, ch.norm_tiles, cls.stream);
+        }
     }
     cudaGraph_t graph = nullptr;
     const cudaError_t end = cudaStreamEndCapture(cls.stream, &graph);
@@ -520,14 +594,11 @@ int vsfeel_bm3d_batch_run(vsfeel_bm3d_batch* b, void* stream) {
     cudaSetDevice(b->device);
     int rc = VSFEEL_OK;
     try {
+        // classes one after another on the caller's stream: run side by side,
+        // their persistent launches compete for SMs and L2 (measured slower)
         cudaStream_t st = (cudaStream_t)stream;
+        for (Class& c : b->classes) check(cudaGraphLaunch(c.exec, st), "cudaGraphLaunch");
         check(cudaEventRecord(b->start, st), "cudaEventRecord");
-        for (Class& c : b->classes) {
-            check(cudaStreamWaitEvent(c.stream, b->start, 0), "cudaStreamWaitEvent");
-            check(cudaGraphLaunch(c.exec, c.stream), "cudaGraphLaunch");
-            check(cudaEventRecord(c.done, c.stream), "cudaEventRecord");
-            check(cudaStreamWaitEvent(st, c.done, 0), "cudaStreamWaitEvent");
-        }
     } catch (const Fail& f) {
         rc = error(f.code, f.msg);
     }
@@ -540,9 +611,7 @@ int vsfeel_bm3d_batch_finish(vsfeel_bm3d_batch* b) {
     int prev = -1;
     cudaGetDevice(&prev);
     cudaSetDevice(b->device);
-    int rc = VSFEEL_OK;
-    for (Class& c : b->classes)
-        if (rc == VSFEEL_OK) rc = wait_stream(c.stream);
+    int rc = wait_event(b->start);
     if (rc == VSFEEL_OK) {
         int word = 0;
         cudaError_t e = cudaMemcpy(&word, b->status.p, sizeof(int), cudaMemcpyDeviceToHost);
