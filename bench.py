@@ -170,7 +170,7 @@ GRAD_WORKLOADS = {
 }
 
 
-def time_fwd_bwd(torch, dev, name, steps, warmup):
+def time_fwd_bwd(torch, dev, name, steps, warmup, frames=None):
     """Forward alone (the plain path) and forward+backward through the
     autograd Function on one workload, timed with CUDA events; loss =
     sum(W * out) with W ~ N(0, 1) seeded."""
@@ -179,7 +179,7 @@ def time_fwd_bwd(torch, dev, name, steps, warmup):
     from vsfeel.synthetic import make_clip_device
 
     wl = GRAD_WORKLOADS[name]
-    n, h, w = wl["frames"], wl["height"], wl["width"]
+    n, h, w = frames or wl["frames"], wl["height"], wl["width"]
     x = make_clip_device(n, h, w, sigma=wl["params"]["sigma"], shift=wl["shift"], seed=wl["seed"],
                          device=dev)
     weights = torch.randn(x.shape, generator=torch.Generator(device=dev).manual_seed(6),
@@ -372,9 +372,22 @@ def main() -> int:
     ap.add_argument("--no-grad", action="store_true",
                     help="skip the forward+backward measurements")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--case", choices=sorted(GRAD_WORKLOADS),
+                    help="only time forward and forward+backward of this workload (a small "
+                         "profiling target) and print its line")
+    ap.add_argument("--case-frames", type=int, default=None,
+                    help="frames of the --case clip (default: the workload's)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.case:
+        import torch
+
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+        torch.cuda.set_device(dev)
+        line = time_fwd_bwd(torch, dev, args.case, args.steps, args.warmup, args.case_frames)
+        print(json.dumps(line), flush=True)
+        return 0
 
     import numpy as np
     import torch
