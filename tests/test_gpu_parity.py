@@ -204,3 +204,37 @@ def test_frame_shards_match_whole_clip():
     parts = [shard.denoise_shard(frames, s, shard.cuda_denoiser(params))
              for s in shard.plan(9, 3, params["radius"])]
     assert float(np.abs(np.concatenate(parts) - whole).max()) <= TYPICAL_TOL
+
+
+def test_host_entry_point_with_pinned_buffers_and_mixed_streams():
+    """Pinned host buffers take the overlapped path (uploads and downloads on
+    their own streams); a device call on another stream just before, not
+    synchronised, must not disturb it."""
+    import torch
+
+    params = dict(sigma=5.0, block_step=4, bm_range=12, radius=2, ps_num=2, ps_range=5)
+    frames = make_clip(7, 96, 128, sigma=5.0, shift=3, seed=51)
+    node = _node(frames, **params)
+    ctx = node._ctx
+    src = torch.from_numpy(frames).pin_memory()
+    out = torch.full(frames.shape, float("nan")).pin_memory()
+    dev = torch.from_numpy(frames).cuda()
+    dev_out = torch.empty_like(dev)
+    side = torch.cuda.Stream()
+    with torch.cuda.stream(side):
+        node.output_device(dev, dev_out)
+    rc = ctx.lib.vsfeel_bm3d_process_host(
+        ctx.handle, src.data_ptr(), src.stride(0) * 4, src.stride(1) * 4, out.data_ptr(),
+        out.stride(0) * 4, out.stride(1) * 4, 0, 7)
+    assert rc == _lib.OK, _lib.last_error(ctx.lib)
+    torch.cuda.synchronize()
+    expected = _node(frames, **params).output()
+    assert float(np.abs(out.numpy() - expected).max()) <= TYPICAL_TOL
+    assert float(np.abs(dev_out.cpu().numpy() - expected).max()) <= TYPICAL_TOL
+    # a sub-range, pinned again
+    part = torch.full((3, 96, 128), float("nan")).pin_memory()
+    rc = ctx.lib.vsfeel_bm3d_process_host(
+        ctx.handle, src.data_ptr(), src.stride(0) * 4, src.stride(1) * 4, part.data_ptr(),
+        part.stride(0) * 4, part.stride(1) * 4, 2, 3)
+    assert rc == _lib.OK
+    assert float(np.abs(part.numpy() - expected[2:5]).max()) <= TYPICAL_TOL

@@ -42,6 +42,9 @@ struct StackJob {
 };
 
 // Per-output normalisation: numerator plane read at aggregation step i.
+// The planes' rows (src_pitch floats) are padded to a multiple of 32 floats
+// and their bases 16-byte aligned: the kernel reads them four floats at a
+// time.
 struct NormalizeJob {
     const float* num[kMaxTW];
     int64_t den_offset;  // floats from a numerator plane to its weight plane
@@ -52,7 +55,7 @@ struct NormalizeJob {
 };
 
 // Many normalisations in one launch: output j covers the items
-// tile_first[j] .. tile_first[j+1]-1, one 32x8-pixel tile each.
+// tile_first[j] .. tile_first[j+1]-1, one 128x8-pixel tile each.
 struct NormalizeBatch {
     const NormalizeJob* jobs;
     const int* tile_first;
@@ -120,7 +123,7 @@ inline int filter_items(int nblocks) { return (nblocks + 15) / 16; }
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream);
 cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream);
 cudaError_t launch_normalize_batch(const NormalizeBatch& work, int total_tiles, cudaStream_t stream);
-inline int normalize_tiles(int width, int height) { return ((width + 31) / 32) * ((height + 7) / 8); }
+inline int normalize_tiles(int width, int height) { return ((width + 127) / 128) * ((height + 7) / 8); }
 
 __host__ __device__ inline int block_count(int extent, int step) {
     return (extent - 9 + 2 * step) / step;  // positions x0 = b*step < extent - 8 + step

@@ -260,6 +260,39 @@ struct vsfeel_bm3d {
     DevBuf<float> frames;     // staged input frames (host and frame paths)
     DevBuf<float> outbuf;     // staged output frames (host and frame paths)
     DevBuf<int> status;       // kernels' internal-error word
+    // host path: uploads and downloads on streams of their own, ordered
+    // against the compute stream by per-frame events
+    cudaStream_t up_stream = nullptr, down_stream = nullptr;
+    std::vector<cudaEvent_t> frame_events, out_events;
+
+    // The end of the context's last enqueued work, on whatever stream it
+    // ran: the next call's streams wait for it first, so calls on different
+    // streams, or after a bounded wait gave up, never overlap on the
+    // context's buffers.
+    cudaEvent_t tail = nullptr;
+    bool tail_set = false;
+    void after_prior(cudaStream_t st) {
+        if (tail_set) VSF_CUDA(cudaStreamWaitEvent(st, tail, 0));
+    }
+    void mark_tail(cudaStream_t st) {
+        if (!tail) VSF_CUDA(cudaEventCreateWithFlags(&tail, cudaEventDisableTiming));
+        VSF_CUDA(cudaEventRecord(tail, st));
+        tail_set = true;
+    }
+
+    void copy_streams(size_t nframes_in, size_t nout) {
+        if (!up_stream) VSF_CUDA(cudaStreamCreateWithFlags(&up_stream, cudaStreamNonBlocking));
+        if (!down_stream) VSF_CUDA(cudaStreamCreateWithFlags(&down_stream, cudaStreamNonBlocking));
+        auto grow = [](std::vector<cudaEvent_t>& v, size_t n) {
+            while (v.size() < n) {
+                cudaEvent_t e;
+                VSF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+                v.push_back(e);
+            }
+        };
+        grow(frame_events, nframes_in);
+        grow(out_events, nout);
+    }
 
     int* status_word() {
         if (!status.p) {
@@ -441,10 +474,14 @@ struct vsfeel_bm3d {
     }
 
     // Denoises outputs [first, first+count) from device frames.
+    // before_stack(m) runs before stack m is launched, after_output(n) after
+    // output n's normalisation is enqueued (the host path's copy overlap).
     void run(const std::function<const float*(int)>& frame_ptr, int in_pitch,
              const std::function<float*(int)>& out_ptr, int out_pitch, int first, int count,
              cudaStream_t st, unsigned char* saved = nullptr,
-             const std::function<const float*(int)>* input_ptr = nullptr) {
+             const std::function<const float*(int)>* input_ptr = nullptr,
+             const std::function<void(int)>* before_stack = nullptr,
+             const std::function<void(int)>* after_output = nullptr) {
         if (count <= 0) return;
         const int r = s.radius;
         const int last = first + count - 1;
@@ -460,10 +497,13 @@ struct vsfeel_bm3d {
                 VSF_CUDA(cudaMemsetAsync(slot_pair(n, 0), 0,
                                          sizeof(float) * (size_t)tw() * 2 * acc_plane, st));
             zeroed = std::max(zeroed, want);
+            if (before_stack) (*before_stack)(m);
             launch_stack(m, frame_ptr, in_pitch, first, last, st, saved, false, input_ptr);
             const int done = (m == m_hi) ? last : std::min(last, m - r);
-            for (int n = finished + 1; n <= done; ++n)
+            for (int n = finished + 1; n <= done; ++n) {
                 launch_normalize(n, out_ptr(n), out_pitch, st, saved);
+                if (after_output) (*after_output)(n);
+            }
             finished = std::max(finished, done);
         }
     }
@@ -580,6 +620,14 @@ void vsfeel_bm3d_free(vsfeel_bm3d* ctx) {
             wait_stream(ctx->stream, timeout_ms());
             cudaStreamDestroy(ctx->stream);
         }
+        for (cudaStream_t cs : {ctx->up_stream, ctx->down_stream})
+            if (cs) {
+                wait_stream(cs, timeout_ms());
+                cudaStreamDestroy(cs);
+            }
+        if (ctx->tail) cudaEventDestroy(ctx->tail);
+        for (cudaEvent_t e : ctx->frame_events) cudaEventDestroy(e);
+        for (cudaEvent_t e : ctx->out_events) cudaEventDestroy(e);
         ctx->ring.release();
         ctx->match_xy.release();
         ctx->match_z.release();
@@ -702,6 +750,7 @@ int process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
         if (ref && ref_frame_stride < ref_row_stride * s.height)
             return fail(VSFEEL_E_ARG, "frame stride smaller than a plane");
         cudaStream_t st = (cudaStream_t)stream;
+        ctx->after_prior(st);
         auto src_at = [&](int f) -> const float* { return src + (size_t)f * src_frame_stride; };
         auto out_at = [&](int n) { return dst + (size_t)(n - first) * dst_frame_stride; };
         if (!ref) {
@@ -713,6 +762,7 @@ int process_device(vsfeel_bm3d* ctx, const float* src, int64_t src_frame_stride,
                      (int)src_row_stride, out_at, (int)dst_row_stride, first, count, st, nullptr,
                      &input);
         }
+        ctx->mark_tail(st);
         return VSFEEL_OK;
     });
 }
@@ -744,31 +794,80 @@ int process_host(vsfeel_bm3d* ctx, const float* src, ptrdiff_t src_frame_stride_
         ctx->frames.ensure(ff * nin * (ref ? 2 : 1));
         ctx->outbuf.ensure(ff * count);
         cudaStream_t st = ctx->stream;
-        auto upload = [&](const float* clip, ptrdiff_t fs, ptrdiff_t rs, float* base) {
-            for (int f = f_lo; f <= f_hi; ++f)
-                VSF_CUDA(cudaMemcpy2DAsync(base + (size_t)(f - f_lo) * ff,
-                                           sizeof(float) * ctx->acc_pitch,
-                                           (const char*)clip + (ptrdiff_t)f * fs, rs, row_bytes,
-                                           s.height, cudaMemcpyHostToDevice, st));
-        };
+        ctx->copy_streams((size_t)nin, (size_t)count);
+        ctx->after_prior(st);
+        ctx->after_prior(ctx->up_stream);
         float* src_base = ctx->frames.p;
         float* ref_base = ctx->frames.p + (size_t)nin * ff;
-        upload(src, src_frame_stride_bytes, src_row_stride_bytes, src_base);
-        if (ref) upload(ref, ref_frame_stride_bytes, ref_row_stride_bytes, ref_base);
-        auto src_at = [&](int f) -> const float* { return src_base + (size_t)(f - f_lo) * ff; };
-        auto out_at = [&](int n) { return ctx->outbuf.p + (size_t)(n - first) * ff; };
-        if (!ref) {
-            ctx->run(src_at, ctx->acc_pitch, out_at, ctx->acc_pitch, first, count, st);
-        } else {
-            const std::function<const float*(int)> input = src_at;
-            ctx->run([&](int f) -> const float* { return ref_base + (size_t)(f - f_lo) * ff; },
-                     ctx->acc_pitch, out_at, ctx->acc_pitch, first, count, st, nullptr, &input);
-        }
-        for (int q = 0; q < count; ++q)
+        // Uploads run on their own stream in frame order, each frame's
+        // completion marked by an event; stack m waits only for the last
+        // frame it reads, clamp(m + r), so the copies overlap the stacks
+        // before it. Frames go up just before the first stack that needs
+        // them, so a pageable source (whose copies block the host) still
+        // overlaps the work already enqueued.
+        int uploaded = f_lo - 1;
+        auto upload_to = [&](int f_need) {
+            for (int f = uploaded + 1; f <= f_need; ++f) {
+                VSF_CUDA(cudaMemcpy2DAsync(src_base + (size_t)(f - f_lo) * ff,
+                                           sizeof(float) * ctx->acc_pitch,
+                                           (const char*)src + (ptrdiff_t)f * src_frame_stride_bytes,
+                                           src_row_stride_bytes, row_bytes, s.height,
+                                           cudaMemcpyHostToDevice, ctx->up_stream));
+                if (ref)
+                    VSF_CUDA(cudaMemcpy2DAsync(ref_base + (size_t)(f - f_lo) * ff,
+                                               sizeof(float) * ctx->acc_pitch,
+                                               (const char*)ref + (ptrdiff_t)f * ref_frame_stride_bytes,
+                                               ref_row_stride_bytes, row_bytes, s.height,
+                                               cudaMemcpyHostToDevice, ctx->up_stream));
+                VSF_CUDA(cudaEventRecord(ctx->frame_events[f - f_lo], ctx->up_stream));
+            }
+            uploaded = std::max(uploaded, f_need);
+        };
+        const std::function<void(int)> before = [&](int m) {
+            const int f_need = std::min(ctx->clampf(m + r), f_hi);
+            upload_to(f_need);
+            VSF_CUDA(cudaStreamWaitEvent(st, ctx->frame_events[f_need - f_lo], 0));
+        };
+        // Downloads: into page-locked memory each output goes down as soon as
+        // it is normalised; into pageable memory (whose copies would block the
+        // host until the output exists) all of them after the last stack.
+        cudaPointerAttributes pa{};
+        const bool pinned_dst = cudaPointerGetAttributes(&pa, dst) == cudaSuccess &&
+                                pa.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        auto download = [&](int n, cudaStream_t cs) {
+            const int q = n - first;
             VSF_CUDA(cudaMemcpy2DAsync((char*)dst + (ptrdiff_t)q * dst_frame_stride_bytes,
                                        dst_row_stride_bytes, ctx->outbuf.p + (size_t)q * ff,
                                        sizeof(float) * ctx->acc_pitch, row_bytes, s.height,
-                                       cudaMemcpyDeviceToHost, st));
+                                       cudaMemcpyDeviceToHost, cs));
+        };
+        const std::function<void(int)> after = [&](int n) {
+            VSF_CUDA(cudaEventRecord(ctx->out_events[n - first], st));
+            VSF_CUDA(cudaStreamWaitEvent(ctx->down_stream, ctx->out_events[n - first], 0));
+            download(n, ctx->down_stream);
+        };
+        auto src_at = [&](int f) -> const float* { return src_base + (size_t)(f - f_lo) * ff; };
+        auto out_at = [&](int n) { return ctx->outbuf.p + (size_t)(n - first) * ff; };
+        const std::function<void(int)>* after_ptr = pinned_dst ? &after : nullptr;
+        if (!ref) {
+            ctx->run(src_at, ctx->acc_pitch, out_at, ctx->acc_pitch, first, count, st, nullptr,
+                     nullptr, &before, after_ptr);
+        } else {
+            const std::function<const float*(int)> input = src_at;
+            ctx->run([&](int f) -> const float* { return ref_base + (size_t)(f - f_lo) * ff; },
+                     ctx->acc_pitch, out_at, ctx->acc_pitch, first, count, st, nullptr, &input,
+                     &before, after_ptr);
+        }
+        if (!pinned_dst)
+            for (int n = first; n < first + count; ++n) download(n, st);
+        // the context's work ends when both the compute and download streams do
+        cudaEvent_t down_end = ctx->out_events[count - 1];
+        VSF_CUDA(cudaEventRecord(down_end, ctx->down_stream));
+        VSF_CUDA(cudaStreamWaitEvent(st, down_end, 0));
+        ctx->mark_tail(st);
+        const int wrc = wait_stream(ctx->down_stream, timeout_ms());
+        if (wrc != VSFEEL_OK) return wrc;
         return ctx->finish(st);
     });
 }
@@ -801,6 +900,7 @@ int get_frame(vsfeel_bm3d* ctx, int n, bool with_ref,
         ctx->frames.ensure(ff * cap * planes);
         ctx->outbuf.ensure(ff);
         cudaStream_t st = ctx->stream;
+        ctx->after_prior(st);
         // evict cached frames outside the window, then upload the missing ones
         for (auto it = ctx->frame_slot.begin(); it != ctx->frame_slot.end();) {
             if (it->first < f_lo || it->first > f_hi) {
@@ -850,6 +950,7 @@ int get_frame(vsfeel_bm3d* ctx, int n, bool with_ref,
         }
         VSF_CUDA(cudaMemcpy2DAsync(dst, dst_stride_bytes, ctx->outbuf.p, sizeof(float) * ctx->acc_pitch,
                                    row_bytes, s.height, cudaMemcpyDeviceToHost, st));
+        ctx->mark_tail(st);
         return ctx->finish(st);
     });
 }
@@ -908,9 +1009,11 @@ int vsfeel_bm3d_forward_saved(vsfeel_bm3d* ctx, const float* src, int64_t src_fr
         if (src_frame_stride < src_row_stride * s.height || dst_frame_stride < dst_row_stride * s.height)
             return fail(VSFEEL_E_ARG, "frame stride smaller than a plane");
         cudaStream_t st = (cudaStream_t)stream;
+        ctx->after_prior(st);
         ctx->run([&](int f) { return src + (size_t)f * src_frame_stride; }, (int)src_row_stride,
                  [&](int n) { return dst + (size_t)n * dst_frame_stride; }, (int)dst_row_stride, 0,
                  s.nframes, st, static_cast<unsigned char*>(saved));
+        ctx->mark_tail(st);
         return VSFEEL_OK;
     });
 }
@@ -932,6 +1035,7 @@ int vsfeel_bm3d_backward(vsfeel_bm3d* ctx, const void* saved, const float* grad_
         if (go_frame_stride < go_row_stride * s.height || gi_frame_stride < gi_row_stride * s.height)
             return fail(VSFEEL_E_ARG, "frame stride smaller than a plane");
         cudaStream_t st = (cudaStream_t)stream;
+        ctx->after_prior(st);
         const auto L = ctx->saved_layout();
         const auto* base = static_cast<const unsigned char*>(saved);
         // the input gradient is accumulated: clear it first (rows may be padded)
@@ -967,6 +1071,7 @@ int vsfeel_bm3d_backward(vsfeel_bm3d* ctx, const void* saved, const float* grad_
         job.height = s.height;
         ctx->traced(VSFEEL_KERNEL_ADJOINT, st, [&] { return launch_adjoint(job, st); });
         ctx->launches += 1;
+        ctx->mark_tail(st);
         return VSFEEL_OK;
     });
 }
@@ -1027,12 +1132,14 @@ int vsfeel_bm3d_match_table_device(vsfeel_bm3d* ctx, const float* src, int64_t s
         ctx->match_xy.ensure((size_t)ctx->nblocks * 8);
         ctx->match_z.ensure((size_t)ctx->nblocks);
         cudaStream_t st = ctx->stream;
+        ctx->after_prior(st);
         // outputs range empty: the filter runs but every slice is dropped
         ctx->launch_stack(m, [&](int f) { return src + (size_t)f * src_frame_stride; },
                           (int)src_row_stride, 1, 0, st, nullptr, true);
         std::vector<uint32_t> xy((size_t)ctx->nblocks * 8), zz((size_t)ctx->nblocks);
         VSF_CUDA(cudaMemcpyAsync(xy.data(), ctx->match_xy.p, xy.size() * 4, cudaMemcpyDeviceToHost, st));
         VSF_CUDA(cudaMemcpyAsync(zz.data(), ctx->match_z.p, zz.size() * 4, cudaMemcpyDeviceToHost, st));
+        ctx->mark_tail(st);
         const int rc = ctx->finish(st);
         if (rc != VSFEEL_OK) return rc;
         for (int b = 0; b < ctx->nblocks; ++b)

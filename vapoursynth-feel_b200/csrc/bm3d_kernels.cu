@@ -279,18 +279,44 @@ __global__ void __launch_bounds__(128) bm3d_filter_kernel(const StackJob job) {
 }
 
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) bm3d_normalize_kernel(const NormalizeJob job) {
-    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
-    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
-    if (x >= job.width || y >= job.height) return;
-    const size_t o = (size_t)y * job.src_pitch + x;
-    double acc = 0.0, acw = 0.0;
-    for (int i = 0; i < job.tw; ++i) {
-        acc += (double)job.num[i][o];
-        acw += (double)job.num[i][o + job.den_offset];
+// Four consecutive pixels (x0 .. x0+3) of one row: float4 loads from the
+// slices (their rows are padded to 32 floats, so the loads stay inside and
+// aligned), slice pointers indexed statically, each pixel's FP64 sums in
+// the reference's order i = 0..tw-1.
+__device__ __forceinline__ void normalize_px4(const NormalizeJob& job, int x0, int y) {
+    const size_t o = (size_t)y * job.src_pitch + x0;
+    double acc[4] = {0.0, 0.0, 0.0, 0.0}, acw[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int i = 0; i < kMaxTW; ++i) {
+        if (i < job.tw) {
+            const float4 a = *reinterpret_cast<const float4*>(job.num[i] + o);
+            const float4 w = *reinterpret_cast<const float4*>(job.num[i] + o + job.den_offset);
+            acc[0] += (double)a.x;
+            acc[1] += (double)a.y;
+            acc[2] += (double)a.z;
+            acc[3] += (double)a.w;
+            acw[0] += (double)w.x;
+            acw[1] += (double)w.y;
+            acw[2] += (double)w.z;
+            acw[3] += (double)w.w;
+        }
     }
-    job.out[(size_t)y * job.out_pitch + x] = (float)(acc / acw);
-    if (job.den_out) job.den_out[(size_t)y * job.den_pitch + x] = (float)acw;
+    float* out = job.out + (size_t)y * job.out_pitch;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (x0 + k < job.width) {
+            out[x0 + k] = (float)(acc[k] / acw[k]);
+            if (job.den_out) job.den_out[(size_t)y * job.den_pitch + x0 + k] = (float)acw[k];
+        }
+    }
+}
+
+// One CTA: 128 x 8 pixels, 4 per thread.
+__global__ void __launch_bounds__(256) bm3d_normalize_kernel(const NormalizeJob job) {
+    const int x0 = (blockIdx.x * 32 + (threadIdx.x & 31)) * 4;
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (x0 >= job.width || y >= job.height) return;
+    normalize_px4(job, x0, y);
 }
 
 // Batched form: the filter of 16 blocks of one stack per CTA.
@@ -318,7 +344,7 @@ __global__ void __launch_bounds__(128) bm3d_filter_batch_kernel(const FilterBatc
     filter_group<false>(job, b, valid, mxy, job.match_z[b], sub, buf);
 }
 
-// Batched form: one CTA per 32x8 tile of one output frame.
+// Batched form: one CTA per 128x8 tile of one output frame.
 __global__ void __launch_bounds__(256) bm3d_normalize_batch_kernel(const NormalizeBatch work) {
     const int item = blockIdx.x;
     int lo = 0, hi = work.njobs - 1;
@@ -331,17 +357,11 @@ __global__ void __launch_bounds__(256) bm3d_normalize_batch_kernel(const Normali
     }
     const NormalizeJob& job = work.jobs[lo];
     const int t = item - work.tile_first[lo];
-    const int tiles_x = (job.width + 31) / 32;
-    const int x = (t % tiles_x) * 32 + (threadIdx.x & 31);
+    const int tiles_x = (job.width + 127) / 128;
+    const int x0 = ((t % tiles_x) * 32 + (threadIdx.x & 31)) * 4;
     const int y = (t / tiles_x) * 8 + (threadIdx.x >> 5);
-    if (x >= job.width || y >= job.height) return;
-    const size_t o = (size_t)y * job.src_pitch + x;
-    double acc = 0.0, acw = 0.0;
-    for (int i = 0; i < job.tw; ++i) {
-        acc += (double)job.num[i][o];
-        acw += (double)job.num[i][o + job.den_offset];
-    }
-    job.out[(size_t)y * job.out_pitch + x] = (float)(acc / acw);
+    if (x0 >= job.width || y >= job.height) return;
+    normalize_px4(job, x0, y);
 }
 
 // ---------------------------------------------------------------------------
@@ -485,7 +505,7 @@ cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream) {
 }
 
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream) {
-    dim3 grid((job.width + 31) / 32, (job.height + 7) / 8);
+    dim3 grid((job.width + 127) / 128, (job.height + 7) / 8);
     bm3d_normalize_kernel<<<grid, 256, 0, stream>>>(job);
     return cudaGetLastError();
 }
