@@ -57,7 +57,7 @@ namespace {
 constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMinK = 2, kMaxK = 5;
 constexpr int kCollect = 64;                // candidates a block collects per pass
-constexpr int kLaneHits = 8;                // hits a lane holds in registers (first pass)
+constexpr int kLaneChunks = 4;              // chunks with hits a lane notes (first pass)
 constexpr uint64_t kKeyMax = (uint64_t(0x7f7fffffu) << 32) | 0x7fffffffu;  // (FLT_MAX, INT_MAX)
 
 __device__ __forceinline__ uint64_t make_key(float err, int seq) {
@@ -395,24 +395,20 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
     }
     uint64_t tkey = (uint64_t(__float_as_uint(bound)) << 32) | 0xffffffffu;
     int n = 0;
-    // First pass: every lane keeps its hits (error at or below the bound) in
-    // registers as (error, window << 24 | table index) -- a few selects per
-    // hit instead of a division and a shared atomic -- then turns them into
-    // (error, scan index) keys in a loop all lanes run together and places
-    // them by a prefix sum over the group. A group with a lane of more than
-    // kLaneHits hits, or more than kCollect in all, takes the general loop
-    // below (rare).
+    // First pass: the sweep only notes, per lane, which chunks of 16 entries
+    // hold hits (errors at or below the bound) and a hit bitmask for each --
+    // no branch per entry; afterwards every lane expands its noted chunks in
+    // one loop, so the hits of different lanes are handled together, and the
+    // keys are placed by a prefix sum over the group. A group with a lane of
+    // more than kLaneChunks such chunks, or more than kCollect hits in all,
+    // takes the general loop below (rare).
     bool fast = false;
     {
         const float terr = bound;
-        float he[kLaneHits];
-        uint32_t hf[kLaneHits];
+        uint32_t ch[kLaneChunks], cm[kLaneChunks];
 #pragma unroll
-        for (int i = 0; i < kLaneHits; ++i) {
-            he[i] = 0.0f;
-            hf[i] = 0u;
-        }
-        int nh = 0;
+        for (int i = 0; i < kLaneChunks; ++i) ch[i] = cm[i] = 0u;
+        int nc = 0;
         for (int wi = 0; wi < nwin; ++wi) {
             const Window w = wins[wi];
             const int n_w = w.rw * w.h;
@@ -430,25 +426,30 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
                 for (int k = 0; k < 4; ++k)
                     mn = fminf(mn, fminf(fminf(q[k].x, q[k].y), fminf(q[k].z, q[k].w)));
                 if (!(mn <= terr)) continue;
+                uint32_t mask = 0u;
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     const float ev[4] = {q[k].x, q[k].y, q[k].z, q[k].w};
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
                         const int f = 4 * (v0 + sub + 8 * k) + u;
-                        if (f < n_w && ev[u] <= terr && ev[u] < kFltMax) {
-#pragma unroll
-                            for (int i = 0; i < kLaneHits; ++i) {
-                                he[i] = i == nh ? ev[u] : he[i];
-                                hf[i] = i == nh ? (uint32_t(wi) << 24) | uint32_t(f) : hf[i];
-                            }
-                            ++nh;
-                        }
+                        const bool hit = f < n_w && ev[u] <= terr && ev[u] < kFltMax;
+                        mask |= hit ? (1u << (4 * k + u)) : 0u;
                     }
+                }
+                if (mask) {
+#pragma unroll
+                    for (int i = 0; i < kLaneChunks; ++i) {
+                        ch[i] = i == nc ? (uint32_t(wi) << 24) | uint32_t(v0) : ch[i];
+                        cm[i] = i == nc ? mask : cm[i];
+                    }
+                    ++nc;
                 }
             }
         }
-        const int cnt = min(nh, kLaneHits);
+        int cnt = 0;
+#pragma unroll
+        for (int i = 0; i < kLaneChunks; ++i) cnt += __popc(cm[i]);
         int incl = cnt;
 #pragma unroll
         for (int off = 1; off < 8; off <<= 1) {
@@ -456,17 +457,21 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
             if (sub >= off) incl += t;
         }
         const int total = __shfl_sync(gmask, incl, 7, 8);
-        const bool overflow = __any_sync(gmask, nh > kLaneHits) || total > kCollect;
+        const bool overflow = __any_sync(gmask, nc > kLaneChunks) || total > kCollect;
         if (!overflow) {
-            const int excl = incl - cnt;
+            int pos = incl - cnt;
 #pragma unroll
-            for (int i = 0; i < kLaneHits; ++i) {
-                if (i < cnt) {
-                    const Window w = wins[hf[i] >> 24];
-                    const int f = int(hf[i] & 0xffffffu);
+            for (int i = 0; i < kLaneChunks; ++i) {
+                uint32_t m = cm[i];
+                const Window w = wins[ch[i] >> 24];
+                const int v0 = int(ch[i] & 0xffffffu);
+                while (m) {
+                    const int b = __ffs(m) - 1;
+                    m &= m - 1;
+                    const int f = 4 * (v0 + sub + 8 * (b >> 2)) + (b & 3);
                     const int d = f / w.h;
                     const int row = f - d * w.h;
-                    gs->buf[excl + i] = make_key(he[i], w.seq_base + row * w.rw + d);
+                    gs->buf[pos++] = make_key(E[w.eoff + f], w.seq_base + row * w.rw + d);
                 }
             }
             n = total;
