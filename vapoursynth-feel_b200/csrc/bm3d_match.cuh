@@ -372,27 +372,29 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
                             GroupState* gs, unsigned gmask) {
     const int sub = threadIdx.x & 7;
     // bound: the 8th smallest of the rows' two smallest errors -- at least 8
-    // candidates lie at or below it
-    float bound = kFltMax;
+    // candidates lie at or below it. Each lane's list is sorted; three
+    // bitonic merge stages with the lanes 1, 2 and 4 apart leave every lane
+    // with the group's 8 smallest, sorted.
 #pragma unroll
-    for (int r = 0; r < 8; ++r) {
-        float best = lb[0];
-        int src = sub;
+    for (int off = 1; off < 8; off <<= 1) {
+        float o[8];
 #pragma unroll
-        for (int off = 1; off < 8; off <<= 1) {
-            const float o = __shfl_xor_sync(gmask, best, off);
-            const int os = __shfl_xor_sync(gmask, src, off);
-            const bool take = o < best || (o == best && os < src);
-            best = take ? o : best;
-            src = take ? os : src;
-        }
-        bound = best;
-        if (sub == src) {
+        for (int i = 0; i < 8; ++i) o[i] = __shfl_xor_sync(gmask, lb[i], off);
+        // the 8 smallest of both lists form a bitonic sequence ...
 #pragma unroll
-            for (int i = 0; i < 7; ++i) lb[i] = lb[i + 1];
-            lb[7] = kFltMax;
-        }
+        for (int i = 0; i < 8; ++i) lb[i] = fminf(lb[i], o[7 - i]);
+        // ... which three compare-exchange levels sort
+#pragma unroll
+        for (int d = 4; d > 0; d >>= 1)
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                if ((i & d) == 0) {
+                    const float a = lb[i], b = lb[i + d];
+                    lb[i] = fminf(a, b);
+                    lb[i + d] = fmaxf(a, b);
+                }
     }
+    const float bound = lb[7];
     uint64_t tkey = (uint64_t(__float_as_uint(bound)) << 32) | 0xffffffffu;
     int n = 0;
     // First pass: the sweep only notes, per lane, which chunks of 16 entries
@@ -621,23 +623,6 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
         select_top8(E, wins, nwin, lb, gs, gmask);
 }
 
-// global list insertion of a temporal match (src/bm3d.comp:304-322)
-__device__ __forceinline__ void ginsert(float ge[8], uint32_t gxy[8], int gz[8], float err,
-                                        uint32_t cxy, int cz) {
-    if (err < ge[7]) {
-        int pos = 7;
-        while (pos > 0 && err < ge[pos - 1]) {
-            ge[pos] = ge[pos - 1];
-            gxy[pos] = gxy[pos - 1];
-            gz[pos] = gz[pos - 1];
-            --pos;
-        }
-        ge[pos] = err;
-        gxy[pos] = cxy;
-        gz[pos] = cz;
-    }
-}
-
 // Position of a key. Sentinels decode to (0, 0) as in the reference.
 __device__ __forceinline__ uint32_t key_xy(uint64_t key, const Window* wins, int area) {
     if (key == kKeyMax) return 0u;
@@ -769,6 +754,10 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         return s;
     };
 
+    float ge = kFltMax;
+    uint32_t gxy = 0u;
+    int gz = 0;
+
     // spatial search (src/bm3d.comp:479-538)
     {
         const Region s = stage(fc, R);
@@ -777,9 +766,10 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         search_windows<kExact>(s, cur_s, c7, win, 1, E, gs, gmask, job.status);
         const uint64_t k = gs->top[sub];
         const uint32_t xy = key_xy(k, win, 0);
-        gs->ge[sub] = key_err(k);
-        gs->gxy[sub] = xy;
-        gs->gz[sub] = r;
+        // the global match list: lane `sub` holds entry sub
+        ge = key_err(k);
+        gxy = xy;
+        gz = r;
         gs->sxy[sub] = xy;
         __syncwarp(gmask);
     }
@@ -802,49 +792,55 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
             }
             __syncwarp(gmask);
             search_windows<kExact>(s, cur_s, c7, win, P, E, gs, gmask, job.status);
-            if (sub == 0) {
-                for (int i = 0; i < P; ++i) {
-                    const uint64_t k = gs->top[i];
-                    const uint32_t fxy = key_xy(k, win, area);
-                    ginsert(gs->ge, gs->gxy, gs->gz, key_err(k), fxy, z);
-                    gs->pxy[i] = fxy;
+            // the frame's first P matches enter the global list in order with
+            // the reference's strict < (src/bm3d.comp:304-322): an entry goes
+            // after the ones it does not beat; the group's lanes shift in
+            // parallel
+            for (int i = 0; i < P; ++i) {
+                const uint64_t k = gs->top[i];
+                const uint32_t fxy = key_xy(k, win, area);
+                const float err = key_err(k);
+                const float e7 = __shfl_sync(gmask, ge, 7, 8);
+                const unsigned below = __ballot_sync(gmask, ge <= err);
+                const float pe = __shfl_up_sync(gmask, ge, 1, 8);
+                const uint32_t pxy = __shfl_up_sync(gmask, gxy, 1, 8);
+                const int pz = __shfl_up_sync(gmask, gz, 1, 8);
+                if (err < e7) {
+                    const int pos = __popc((below >> (lane & ~7)) & 0xffu);
+                    if (sub > pos) {
+                        ge = pe;
+                        gxy = pxy;
+                        gz = pz;
+                    } else if (sub == pos) {
+                        ge = err;
+                        gxy = fxy;
+                        gz = z;
+                    }
                 }
+                if (sub == 0) gs->pxy[i] = fxy;
             }
             __syncwarp(gmask);
         }
     }
 
-    // forced self-match (src/bm3d.comp:639-663): the final list in gxy/gz
-    if (sub == 0) {
-        uint32_t gxy[8];
-        int gz[8];
-        for (int k = 0; k < 8; ++k) {
-            gxy[k] = gs->gxy[k];
-            gz[k] = gs->gz[k];
-        }
+    // forced self-match (src/bm3d.comp:639-663): when (x, y, r) is not among
+    // the 8, the list shifts right and it enters at slot 0
+    {
         const uint32_t self_xy = uint32_t(x) | (uint32_t(y) << 16);
-        bool has_self = false;
-        for (int k = 0; k < 8; ++k) has_self = has_self || (gxy[k] == self_xy && gz[k] == r);
+        const bool has_self = __any_sync(gmask, gxy == self_xy && gz == r);
+        const uint32_t pxy = __shfl_up_sync(gmask, gxy, 1, 8);
+        const int pz = __shfl_up_sync(gmask, gz, 1, 8);
         if (!has_self) {
-            for (int k = 7; k > 0; --k) {
-                gxy[k] = gxy[k - 1];
-                gz[k] = gz[k - 1];
-            }
-            gxy[0] = self_xy;
-            gz[0] = r;
+            gxy = sub == 0 ? self_xy : pxy;
+            gz = sub == 0 ? r : pz;
         }
-        uint32_t zp = 0;
-        for (int k = 0; k < 8; ++k) {
-            gs->gxy[k] = gxy[k];
-            zp |= uint32_t(gz[k]) << (4 * k);
-        }
-        gs->gz[0] = int(zp);
+        const uint32_t zp = __reduce_or_sync(gmask, uint32_t(gz) << (4 * sub));
+        gs->gxy[sub] = gxy;
+        if (sub == 0) gs->gz[0] = int(zp);
         if (valid && kMode != kFused) {
             const size_t b = (size_t)by * job.nbx + bx;
-            uint4* dst = reinterpret_cast<uint4*>(job.match_xy + b * 8);
-            dst[0] = make_uint4(gxy[0], gxy[1], gxy[2], gxy[3]);
-            dst[1] = make_uint4(gxy[4], gxy[5], gxy[6], gxy[7]);
-            job.match_z[b] = zp;
+            job.match_xy[b * 8 + sub] = gxy;
+            if (sub == 0) job.match_z[b] = zp;
         }
     }
 
