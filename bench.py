@@ -304,6 +304,42 @@ def time_batched(torch, dev, steps, warmup):
             "max_abs_diff_vs_plain_first4": worst, "steps": steps, "warmup": warmup}
 
 
+def time_all_planes(torch, dev, nfr, steps, warmup):
+    """Per-plane denoising (the ``planes`` extension): a YUV420PS 1080p clip
+    with all three planes denoised, the 960x540 chroma planes noisy like
+    luma, same arguments per plane. Device-resident, one stream, CUDA events;
+    Mpx/s counts the pixels of all three planes."""
+    import vsfeel
+    from vsfeel.synthetic import make_clip
+
+    planes = [make_clip(nfr, HEIGHT, WIDTH, sigma=3.0, shift=4, seed=4000),
+              make_clip(nfr, HEIGHT // 2, WIDTH // 2, sigma=3.0, shift=2, seed=4001),
+              make_clip(nfr, HEIGHT // 2, WIDTH // 2, sigma=3.0, shift=2, seed=4002)]
+    node = vsfeel.BM3Dv2(vsfeel.clip_from_array(*planes), planes=[0, 1, 2],
+                         device=dev.index or 0, **PARAMS)
+    src = [torch.from_numpy(x).to(dev) for x in planes]
+    out = [torch.empty_like(x) for x in src]
+
+    def step():
+        for p in range(3):
+            node.output_device(src[p], out[p], plane=p)
+
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        step()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / steps
+    px = sum(x.size for x in planes)
+    return {"workload": f"bm3dv2_all_planes_yuv420ps_1920x1080x{nfr}_r2",
+            "mpx_s": px / ms / 1e3, "ms_per_step": ms, "megapixels_per_step": px / 1e6,
+            "steps": steps, "warmup": warmup}
+
+
 def run_reference(args) -> int:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -372,6 +408,8 @@ def main() -> int:
     ap.add_argument("--no-grad", action="store_true",
                     help="skip the forward+backward measurements")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-form measurement")
+    ap.add_argument("--no-planes", action="store_true",
+                    help="skip the all-planes (chroma denoised) measurement")
     ap.add_argument("--case", choices=sorted(GRAD_WORKLOADS),
                     help="only time forward and forward+backward of this workload (a small "
                          "profiling target) and print its line")
@@ -509,6 +547,8 @@ def main() -> int:
                            for name in GRAD_WORKLOADS]
     if world == 1 and not args.no_batch:
         line["batched"] = time_batched(torch, dev, max(2, args.steps // 3), 3)
+    if world == 1 and not args.no_planes:
+        line["all_planes"] = time_all_planes(torch, dev, nfr, max(3, args.steps // 2), 3)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_port(luma)
     print(json.dumps(line), flush=True)

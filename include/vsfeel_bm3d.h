@@ -88,6 +88,27 @@ VSFEEL_API void vsfeel_bm3d_args_init(vsfeel_bm3d_args* args);
 VSFEEL_API int vsfeel_bm3d_create(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
                        int device, vsfeel_bm3d** out);
 
+/* Per-plane denoising, an extension past the reference: the reference parses
+ * sigma, block_step, bm_range, ps_num and ps_range per plane but applies
+ * element [0] to luma and passes chroma through (src/bm3d.cpp:1090-1167,
+ * 1265-1272). vsfeel_bm3d_create_plane binds a context to plane `plane`
+ * (0 = luma; 1, 2 = the chroma planes of a YUV clip, of size
+ * (width >> sub_sampling_w) x (height >> sub_sampling_h)) with element
+ * [plane] of every array, filled by the reference's rule. Every other entry
+ * point then works on that plane: the fetch callbacks and the host or device
+ * buffers hold plane `plane` of each frame. In the final pass, ref supplies
+ * the same plane. vsfeel_bm3d_create is vsfeel_bm3d_create_plane(.., 0, ..).
+ * Planes narrower or shorter than 8 are rejected. */
+VSFEEL_API int vsfeel_bm3d_create_plane(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
+                             int plane, int device, vsfeel_bm3d** out);
+
+/* The effective parameters (vsfeel_bm3d_info, device_bytes 0) that
+ * vsfeel_bm3d_create_plane would use for `plane`, after the same validation;
+ * no device is touched. */
+struct vsfeel_bm3d_info;
+VSFEEL_API int vsfeel_bm3d_plane_params(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
+                             int plane, struct vsfeel_bm3d_info* info);
+
 /* BM3DFree. Accepts NULL. */
 VSFEEL_API void vsfeel_bm3d_free(vsfeel_bm3d* ctx);
 

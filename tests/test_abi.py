@@ -122,3 +122,78 @@ def test_null_context_is_rejected():
     assert lib.vsfeel_bm3d_frame_range(None, 0, ctypes.byref(lo), ctypes.byref(hi)) == _lib.E_ARG
     lib.vsfeel_bm3d_free(None)
     assert lib.vsfeel_bm3d_launch_count(None) == 0
+
+
+def _yuv420_clip(h=32, w=48, n=4):
+    z = np.zeros
+    return vsfeel.clip_from_array(z((n, h, w), np.float32), z((n, h // 2, w // 2), np.float32),
+                                  z((n, h // 2, w // 2), np.float32))
+
+
+def test_plane_params_follow_the_reference_fill_rule():
+    """Element [p] of each per-plane array, a missing element copying the
+    previous one (src/bm3d.cpp:1090-1167), on the plane's own dimensions."""
+    clip = _yuv420_clip()
+    kw = dict(sigma=[2.0, 4.0], block_step=[8, 4, 2], bm_range=[16], ps_num=[3, 1],
+              ps_range=[7, 5, 3], radius=1)
+    want = {0: (2.0, 8, 16, 3, 7, 48, 32), 1: (4.0, 4, 16, 1, 5, 24, 16),
+            2: (4.0, 2, 16, 1, 3, 24, 16)}
+    for p, (sigma, step, bmr, psn, psr, w, h) in want.items():
+        inf = vsfeel.plane_params(clip, p, **kw)
+        assert (inf.sigma, inf.block_step, inf.bm_range, inf.ps_num, inf.ps_range) == (
+            sigma, step, bmr, psn, psr), p
+        assert (inf.width, inf.height, inf.num_frames, inf.radius) == (w, h, 4, 1), p
+        assert inf.device_bytes == 0
+    # the threshold scales the plane's own sigma by the pass factor
+    basic = vsfeel.plane_params(clip, 1, **kw).threshold
+    assert basic == np.float32(np.float32(4.0) * np.frombuffer(
+        np.uint32(0x3f021bb6).tobytes(), np.float32)[0])
+    ref = vsfeel.plane_params(clip, 2, ref=clip, **kw).threshold
+    assert ref == np.float32(np.float32(4.0) * np.frombuffer(
+        np.uint32(0x3e40c0c1).tobytes(), np.float32)[0])
+
+
+def test_plane_params_plane_zero_equals_create():
+    """Plane 0 of the extension is the reference's (luma) configuration."""
+    clip = vsfeel.clip_from_array(np.zeros((3, 40, 56), np.float32))
+    inf = vsfeel.plane_params(clip, 0, sigma=[5.0, 1.0], block_step=[4, 8])
+    assert (inf.sigma, inf.block_step, inf.bm_range, inf.width, inf.height) == (5.0, 4, 9, 56, 40)
+    assert (inf.blocks_x, inf.blocks_y) == (13, 9)
+
+
+@pytest.mark.parametrize("plane,fmt_yuv", [(1, False), (3, True), (-1, True)])
+def test_plane_outside_the_clip_is_rejected(plane, fmt_yuv):
+    clip = _yuv420_clip() if fmt_yuv else vsfeel.clip_from_array(np.zeros((2, 16, 16), np.float32))
+    with pytest.raises(vsfeel.Error, match='"planes" must name planes of the clip'):
+        vsfeel.plane_params(clip, plane)
+
+
+def test_small_chroma_planes_are_rejected():
+    clip = _yuv420_clip(h=14, w=48)
+    vsfeel.plane_params(clip, 0)
+    with pytest.raises(vsfeel.Error, match="chroma planes must be at least 8x8"):
+        vsfeel.plane_params(clip, 1)
+
+
+def test_plane_params_validate_every_argument():
+    clip = _yuv420_clip()
+    with pytest.raises(vsfeel.Error, match='"block_step" must be in range'):
+        vsfeel.plane_params(clip, 2, block_step=[4, 4, 9])
+
+
+@pytest.mark.parametrize("planes,message", [
+    ([], '"planes" must name at least one plane'),
+    ([0, 0], '"planes" must not repeat a plane'),
+    ([0, 3], '"planes" must name planes of the clip'),
+])
+def test_planes_keyword_validation(planes, message):
+    with pytest.raises(vsfeel.Error, match=re.escape("BM3D: " + message)):
+        vsfeel.BM3Dv2(_yuv420_clip(), planes=planes)
+
+
+def test_all_planes_reach_the_device_check_without_a_gpu():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(vsfeel.Error, match="no CUDA device"):
+        vsfeel.BM3Dv2(_yuv420_clip(), planes=[0, 1, 2], sigma=[3.0, 5.0], block_step=[4, 2])

@@ -106,8 +106,11 @@ struct Settings {
 };
 
 // Argument parsing and validation in the order and with the messages of
-// BM3DCreate (src/bm3d.cpp:1062-1190, 1257-1275).
-int parse_args(const vsfeel_bm3d_args* a, const vsfeel_bm3d_video_info* vi, Settings& s) {
+// BM3DCreate (src/bm3d.cpp:1062-1190, 1257-1275). `plane` selects which
+// element of the per-plane arrays applies and which plane's dimensions the
+// context works on; the reference itself always uses element [0] on luma.
+int parse_args(const vsfeel_bm3d_args* a, const vsfeel_bm3d_video_info* vi, Settings& s,
+               int plane = 0) {
     if (!a || !vi) return fail(VSFEEL_E_ARG, "null argument");
     if (a->has_ref) {
         const vsfeel_bm3d_video_info* r = a->ref_info;
@@ -176,18 +179,6 @@ int parse_args(const vsfeel_bm3d_args* a, const vsfeel_bm3d_video_info* vi, Sett
     if (s.num_streams <= 0) return fail(VSFEEL_E_ARG, "\"num_streams\" must be positive");
     const int ext = a->extractor_exp_set ? a->extractor_exp : 0;
 
-    s.sigma = sigma[0];
-    s.final_pass = a->has_ref != 0;
-    s.thr = sigma[0] * sigma_factor(s.final_pass);
-    s.extractor = ext != 0 ? std::ldexp(1.0f, ext) : 0.0f;
-    s.step = step[0];
-    s.bm_range = bmr[0];
-    s.ps_num = psn[0];
-    s.ps_range = psr[0];
-    s.width = vi->width;
-    s.height = vi->height;
-    s.nframes = vi->num_frames;
-
     if (vi->color_family == VSFEEL_CF_GRAY) {
         s.chroma = false;
     } else if (vi->color_family == VSFEEL_CF_YUV) {
@@ -195,10 +186,32 @@ int parse_args(const vsfeel_bm3d_args* a, const vsfeel_bm3d_video_info* vi, Sett
     } else {
         return fail(VSFEEL_E_FORMAT, "only Gray and YUV input are currently supported");
     }
+    if (plane < 0 || plane >= (s.chroma ? 3 : 1))
+        return fail(VSFEEL_E_ARG, "\"planes\" must name planes of the clip");
+    if (plane > 0 && (vi->sub_sampling_w < 0 || vi->sub_sampling_w > 4 ||
+                      vi->sub_sampling_h < 0 || vi->sub_sampling_h > 4))
+        return fail(VSFEEL_E_FORMAT, "invalid chroma subsampling");
+
+    // a ref-pass threshold uses the same element as the plane's sigma
+    // (src/bm3d.cpp:1090-1113 scales all three)
+    s.sigma = sigma[plane];
+    s.final_pass = a->has_ref != 0;
+    s.thr = sigma[plane] * sigma_factor(s.final_pass);
+    s.extractor = ext != 0 ? std::ldexp(1.0f, ext) : 0.0f;
+    s.step = step[plane];
+    s.bm_range = bmr[plane];
+    s.ps_num = psn[plane];
+    s.ps_range = psr[plane];
+    // chroma plane sizes as VapourSynth derives them: width >> ssw
+    s.width = plane > 0 ? vi->width >> vi->sub_sampling_w : vi->width;
+    s.height = plane > 0 ? vi->height >> vi->sub_sampling_h : vi->height;
+    s.nframes = vi->num_frames;
+
     // The reference reads outside the plane below 8x8; the match table packs
     // coordinates in 16 bits.
     if (s.width < 8 || s.height < 8)
-        return fail(VSFEEL_E_FORMAT, "clip dimensions must be at least 8x8");
+        return fail(VSFEEL_E_FORMAT, plane > 0 ? "chroma planes must be at least 8x8"
+                                               : "clip dimensions must be at least 8x8");
     if (s.width > 65535 || s.height > 65535)
         return fail(VSFEEL_E_FORMAT, "clip dimensions must be at most 65535");
     if (s.nframes <= 0) return fail(VSFEEL_E_FORMAT, "clip must have at least one frame");
@@ -542,9 +555,9 @@ namespace vsfeel {
 // parameters, without touching the device (used by the allocation-free entry
 // point in bm3d_noalloc.cu).
 int parse_to_info(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
-                  vsfeel_bm3d_info* info) {
+                  vsfeel_bm3d_info* info, int plane) {
     Settings s;
-    const int rc = parse_args(args, vi, s);
+    const int rc = parse_args(args, vi, s, plane);
     if (rc != VSFEEL_OK) return rc;
     std::memset(info, 0, sizeof(*info));
     info->width = s.width;
@@ -580,11 +593,23 @@ void vsfeel_bm3d_args_init(vsfeel_bm3d_args* a) {
 
 int vsfeel_bm3d_create(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi, int device,
                        vsfeel_bm3d** out) {
+    return vsfeel_bm3d_create_plane(args, vi, 0, device, out);
+}
+
+int vsfeel_bm3d_plane_params(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
+                             int plane, vsfeel_bm3d_info* info) {
+    g_error.clear();
+    if (!info) return fail(VSFEEL_E_ARG, "null argument");
+    return vsfeel::parse_to_info(args, vi, info, plane);
+}
+
+int vsfeel_bm3d_create_plane(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
+                             int plane, int device, vsfeel_bm3d** out) {
     g_error.clear();
     if (!out) return fail(VSFEEL_E_ARG, "null output pointer");
     *out = nullptr;
     Settings s;
-    const int rc = parse_args(args, vi, s);
+    const int rc = parse_args(args, vi, s, plane);
     if (rc != VSFEEL_OK) return rc;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {

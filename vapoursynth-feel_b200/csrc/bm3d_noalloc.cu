@@ -33,7 +33,7 @@
 namespace vsfeel {
 
 int parse_to_info(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
-                  vsfeel_bm3d_info* info);
+                  vsfeel_bm3d_info* info, int plane = 0);
 int set_error(int code, const char* msg);
 
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;

@@ -7,6 +7,12 @@ src/bm3d.cpp:1558-1574). Clips are ``VideoNode`` objects holding float32
 planes; ``clip_from_array`` builds one from numpy arrays. Errors raise
 ``vsfeel.Error`` with the reference's messages.
 
+One keyword goes past the reference: ``planes`` (default ``[0]``, the
+reference's behaviour of denoising luma and passing chroma through) lists
+the planes to denoise, each with its own element of the per-plane argument
+arrays, which the reference parses but does not apply
+(src/bm3d.cpp:1090-1167).
+
 All denoising runs in libvsfeel_bm3d.so on the GPU through the C ABI of
 include/vsfeel_bm3d.h; there is no CPU path.
 """
@@ -22,7 +28,7 @@ import numpy as np
 from . import _lib
 
 __all__ = ["Error", "VideoFormat", "GRAYS", "YUV420PS", "YUV444PS", "VideoNode", "VideoFrame",
-           "clip_from_array", "BM3Dv2", "bm3d_device"]
+           "clip_from_array", "BM3Dv2", "bm3d_device", "plane_params"]
 
 
 class Error(Exception):
@@ -137,14 +143,15 @@ def _make_args(ref, sigma, block_step, bm_range, radius, ps_num, ps_range, num_s
 
 
 class _Context:
-    """Owns one vsfeel_bm3d context."""
+    """Owns one vsfeel_bm3d context, bound to one plane of the clip."""
 
-    def __init__(self, clip: VideoNode, args: _lib.Args, device: int):
+    def __init__(self, clip: VideoNode, args: _lib.Args, device: int, plane: int = 0):
         self.lib = _lib.load()
         self.vi = clip.video_info()
+        self.plane = plane
         h = ctypes.c_void_p()
-        rc = self.lib.vsfeel_bm3d_create(ctypes.byref(args), ctypes.byref(self.vi), device,
-                                         ctypes.byref(h))
+        rc = self.lib.vsfeel_bm3d_create_plane(ctypes.byref(args), ctypes.byref(self.vi), plane,
+                                               device, ctypes.byref(h))
         if rc != _lib.OK:
             raise Error(_lib.last_error(self.lib))
         self.handle = h
@@ -167,24 +174,43 @@ class _Context:
 
 class BM3DNode(VideoNode):
     """The filter's output clip. Frames are denoised on demand (``get_frame``,
-    the VapourSynth request path) or all at once (``output``)."""
+    the VapourSynth request path) or all at once (``output``). Each denoised
+    plane has its own context; the others pass through."""
 
-    def __init__(self, clip: VideoNode, ctx: _Context, ref: VideoNode | None = None):
+    def __init__(self, clip: VideoNode, ctxs: Sequence[_Context], ref: VideoNode | None = None):
         super().__init__([clip.plane_array(p) for p in range(clip.format.num_planes)], clip.format)
         self._src = clip
-        self._ctx = ctx
-        self._luma_src = np.ascontiguousarray(clip.plane_array(0), dtype=np.float32)
+        self._ctxs = {c.plane: c for c in ctxs}
+        self._ctx = ctxs[0]
+        self._plane_src = {p: np.ascontiguousarray(clip.plane_array(p), dtype=np.float32)
+                           for p in self._ctxs}
         # the final (Wiener) pass: the basic estimate that matching runs on
-        self._luma_ref = (None if ref is None
-                          else np.ascontiguousarray(ref.plane_array(0), dtype=np.float32))
+        self._plane_ref = (None if ref is None else
+                           {p: np.ascontiguousarray(ref.plane_array(p), dtype=np.float32)
+                            for p in self._ctxs})
+
+    @property
+    def planes(self) -> list[int]:
+        """The denoised planes, in the order given."""
+        return list(self._ctxs)
 
     @property
     def final_pass(self) -> bool:
-        return self._luma_ref is not None
+        return self._plane_ref is not None
 
     @property
     def info(self) -> _lib.Info:
         return self._ctx.info()
+
+    def plane_info(self, plane: int) -> _lib.Info:
+        return self._plane_ctx(plane).info()
+
+    def _plane_ctx(self, plane: int | None) -> _Context:
+        if plane is None:
+            return self._ctx
+        if plane not in self._ctxs:
+            raise Error(f"BM3D: plane {plane} is not denoised by this node")
+        return self._ctxs[plane]
 
     def frame_range(self, n: int) -> tuple[int, int]:
         lo, hi = ctypes.c_int(), ctypes.c_int()
@@ -195,10 +221,16 @@ class BM3DNode(VideoNode):
     def get_frame(self, n: int) -> VideoFrame:
         if not 0 <= n < self.num_frames:
             raise Error("frame index out of range")
-        src = self._luma_src
-        out = np.empty((self.height, self.width), dtype=np.float32)
+        planes = [self._denoise_plane(n, p) if p in self._ctxs else self._src.plane_array(p)[n]
+                  for p in range(self.format.num_planes)]
+        return VideoFrame(planes, self.format)
+
+    def _denoise_plane(self, n: int, plane: int) -> np.ndarray:
+        ctx = self._ctxs[plane]
+        src = self._plane_src[plane]
+        out = np.empty(src.shape[1:], dtype=np.float32)
         if self.final_pass:
-            clips = (src, self._luma_ref)
+            clips = (src, self._plane_ref[plane])
 
             @_lib.FETCH2_FN
             def fetch2(user, clip, f, stride):
@@ -209,8 +241,8 @@ class BM3DNode(VideoNode):
             def release2(user, clip, f):
                 pass
 
-            self._ctx.check(self._ctx.lib.vsfeel_bm3d_get_frame_ref(
-                self._ctx.handle, n, fetch2, release2, None, out.ctypes.data, out.strides[0]))
+            ctx.check(ctx.lib.vsfeel_bm3d_get_frame_ref(
+                ctx.handle, n, fetch2, release2, None, out.ctypes.data, out.strides[0]))
         else:
             @_lib.FETCH_FN
             def fetch(user, f, stride):
@@ -221,20 +253,20 @@ class BM3DNode(VideoNode):
             def release(user, f):
                 pass
 
-            self._ctx.check(self._ctx.lib.vsfeel_bm3d_get_frame(
-                self._ctx.handle, n, fetch, release, None, out.ctypes.data, out.strides[0]))
-        planes = [out] + [self._src.plane_array(p)[n] for p in range(1, self.format.num_planes)]
-        return VideoFrame(planes, self.format)
+            ctx.check(ctx.lib.vsfeel_bm3d_get_frame(
+                ctx.handle, n, fetch, release, None, out.ctypes.data, out.strides[0]))
+        return out
 
     def output_device(self, src, out, first: int = 0, count: int | None = None,
-                      ref=None) -> None:
+                      ref=None, plane: int | None = None) -> None:
         """Denoises from device memory: src is a CUDA float32 tensor
-        (num_frames, H, W) holding the clip's luma, out receives frames
-        first..first+count-1 as (count, H, W); in the final pass ref holds the
-        basic estimate's luma like src. Enqueued on torch's current stream;
-        no host copies."""
+        (num_frames, h, w) holding one plane of the clip (the first denoised
+        plane, or ``plane``), out receives frames first..first+count-1 as
+        (count, h, w); in the final pass ref holds the basic estimate's
+        plane like src. Enqueued on torch's current stream; no host copies."""
         import torch
 
+        ctx = self._plane_ctx(plane)
         count = self.num_frames - first if count is None else count
         for t in (src, out) + ((ref,) if ref is not None else ()):
             if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32
@@ -242,12 +274,12 @@ class BM3DNode(VideoNode):
                 raise Error("BM3D: device buffers must be CUDA float32 (N, H, W) tensors")
         stream = torch.cuda.current_stream(src.device).cuda_stream
         if ref is None:
-            self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_device(
-                self._ctx.handle, src.data_ptr(), src.stride(0), src.stride(1), out.data_ptr(),
+            ctx.check(ctx.lib.vsfeel_bm3d_process_device(
+                ctx.handle, src.data_ptr(), src.stride(0), src.stride(1), out.data_ptr(),
                 out.stride(0), out.stride(1), first, count, stream))
         else:
-            self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_device_ref(
-                self._ctx.handle, src.data_ptr(), src.stride(0), src.stride(1), ref.data_ptr(),
+            ctx.check(ctx.lib.vsfeel_bm3d_process_device_ref(
+                ctx.handle, src.data_ptr(), src.stride(0), src.stride(1), ref.data_ptr(),
                 ref.stride(0), ref.stride(1), out.data_ptr(), out.stride(0), out.stride(1), first,
                 count, stream))
 
@@ -266,39 +298,80 @@ class BM3DNode(VideoNode):
         return {name: (ms[k], n[k]) for k, name in enumerate(_lib.KERNEL_NAMES)}
 
     def output(self, first: int = 0, count: int | None = None,
-               out: np.ndarray | None = None) -> np.ndarray:
-        """Denoised luma of frames first..first+count-1 as (count, H, W)."""
+               out: np.ndarray | None = None, plane: int | None = None) -> np.ndarray:
+        """Denoised frames first..first+count-1 of the first denoised plane
+        (luma by default), or of ``plane``, as (count, h, w)."""
+        ctx = self._plane_ctx(plane)
         count = self.num_frames - first if count is None else count
+        src = self._plane_src[ctx.plane]
         if out is None:
-            out = np.empty((count, self.height, self.width), dtype=np.float32)
-        src = self._luma_src
+            out = np.empty((count,) + src.shape[1:], dtype=np.float32)
         if self.final_pass:
-            ref = self._luma_ref
-            self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_host_ref(
-                self._ctx.handle, src.ctypes.data, src.strides[0], src.strides[1], ref.ctypes.data,
+            ref = self._plane_ref[ctx.plane]
+            ctx.check(ctx.lib.vsfeel_bm3d_process_host_ref(
+                ctx.handle, src.ctypes.data, src.strides[0], src.strides[1], ref.ctypes.data,
                 ref.strides[0], ref.strides[1], out.ctypes.data, out.strides[0], out.strides[1],
                 first, count))
         else:
-            self._ctx.check(self._ctx.lib.vsfeel_bm3d_process_host(
-                self._ctx.handle, src.ctypes.data, src.strides[0], src.strides[1],
+            ctx.check(ctx.lib.vsfeel_bm3d_process_host(
+                ctx.handle, src.ctypes.data, src.strides[0], src.strides[1],
                 out.ctypes.data, out.strides[0], out.strides[1], first, count))
         return out
 
 
+def _plane_list(planes) -> list[int]:
+    if planes is None:
+        return [0]
+    vals = [int(p) for p in (planes if isinstance(planes, (list, tuple, np.ndarray)) else [planes])]
+    if not vals:
+        raise Error('BM3D: "planes" must name at least one plane')
+    if len(set(vals)) != len(vals):
+        raise Error('BM3D: "planes" must not repeat a plane')
+    return vals
+
+
 def BM3Dv2(clip: VideoNode, ref: VideoNode | None = None, sigma=None, block_step=None,
            bm_range=None, radius=None, ps_num=None, ps_range=None, num_streams=None,
-           extractor_exp=None, device: int = 0) -> BM3DNode:
+           extractor_exp=None, planes=None, device: int = 0) -> BM3DNode:
     """core.vsfeel.BM3Dv2: the BM3D basic estimate (hard thresholding), or
-    with ``ref`` (a basic estimate of the same clip) the final Wiener pass."""
+    with ``ref`` (a basic estimate of the same clip) the final Wiener pass.
+    ``planes`` (an extension) lists the planes to denoise; plane p uses
+    element [p] of sigma, block_step, bm_range, ps_num and ps_range."""
     if not isinstance(clip, VideoNode):
         clip = clip_from_array(np.asarray(clip))
     if ref is not None and not isinstance(ref, VideoNode):
         ref = clip_from_array(np.asarray(ref))
     args, keep = _make_args(ref, sigma, block_step, bm_range, radius, ps_num, ps_range,
                             num_streams, extractor_exp)
-    ctx = _Context(clip, args, device)
+    plane_list = _plane_list(planes)
+    # every plane's arguments are checked before any context takes the device
+    lib = _lib.load()
+    vi = clip.video_info()
+    for p in plane_list[1:]:
+        if lib.vsfeel_bm3d_plane_params(ctypes.byref(args), ctypes.byref(vi), p,
+                                        ctypes.byref(_lib.Info())) != _lib.OK:
+            raise Error(_lib.last_error(lib))
+    ctxs = [_Context(clip, args, device, p) for p in plane_list]
     del keep
-    return BM3DNode(clip, ctx, ref)
+    return BM3DNode(clip, ctxs, ref)
+
+
+def plane_params(clip: VideoNode, plane: int = 0, ref: VideoNode | None = None, sigma=None,
+                 block_step=None, bm_range=None, radius=None, ps_num=None, ps_range=None,
+                 num_streams=None, extractor_exp=None) -> _lib.Info:
+    """The parameters ``BM3Dv2(..., planes=[plane])`` applies to ``plane``,
+    validated like BM3DCreate; needs no GPU."""
+    args, keep = _make_args(ref, sigma, block_step, bm_range, radius, ps_num, ps_range,
+                            num_streams, extractor_exp)
+    lib = _lib.load()
+    vi = clip.video_info()
+    inf = _lib.Info()
+    rc = lib.vsfeel_bm3d_plane_params(ctypes.byref(args), ctypes.byref(vi), plane,
+                                      ctypes.byref(inf))
+    del keep
+    if rc != _lib.OK:
+        raise Error(_lib.last_error(lib))
+    return inf
 
 
 def bm3d_device(frames, sigma=None, block_step=None, bm_range=None, radius=None, ps_num=None,

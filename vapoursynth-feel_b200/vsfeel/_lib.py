@@ -18,6 +18,8 @@ LIB_PATH = HERE / "libvsfeel_bm3d.so"
 EXPORTS = (
     "vsfeel_bm3d_args_init",
     "vsfeel_bm3d_create",
+    "vsfeel_bm3d_create_plane",
+    "vsfeel_bm3d_plane_params",
     "vsfeel_bm3d_free",
     "vsfeel_bm3d_frame_range",
     "vsfeel_bm3d_get_frame",
@@ -169,6 +171,12 @@ def load(path: str | os.PathLike | None = None) -> ctypes.CDLL:
     lib.vsfeel_bm3d_create.argtypes = [ctypes.POINTER(Args), ctypes.POINTER(VideoInfo), c_int,
                                        ctypes.POINTER(c_p)]
     lib.vsfeel_bm3d_create.restype = c_int
+    lib.vsfeel_bm3d_create_plane.argtypes = [ctypes.POINTER(Args), ctypes.POINTER(VideoInfo), c_int,
+                                             c_int, ctypes.POINTER(c_p)]
+    lib.vsfeel_bm3d_create_plane.restype = c_int
+    lib.vsfeel_bm3d_plane_params.argtypes = [ctypes.POINTER(Args), ctypes.POINTER(VideoInfo), c_int,
+                                             ctypes.POINTER(Info)]
+    lib.vsfeel_bm3d_plane_params.restype = c_int
     lib.vsfeel_bm3d_free.argtypes = [c_p]
     lib.vsfeel_bm3d_free.restype = None
     lib.vsfeel_bm3d_frame_range.argtypes = [c_p, c_int, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]
