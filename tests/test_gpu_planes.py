@@ -113,3 +113,15 @@ def test_final_pass_per_plane_vs_oracle(oracle_lib):
         expected = oracle_lib.bm3d(clip.plane_array(p), _plane_params(p), ref=est[p])
         out = final.output(plane=p)
         assert np.abs(out.astype(np.float64) - expected).max() <= OUT_TOL, p
+
+
+def test_node_as_ref_uses_its_denoised_planes(oracle_lib):
+    """A BM3DNode stands in for a clip: as ``ref`` it supplies its output."""
+    clip = _yuv420(n=4, seed=95)
+    basic = vsfeel.BM3Dv2(clip, planes=[0, 2], **PLANE_ARGS)
+    assert np.array_equal(basic.plane_array(1), clip.plane_array(1))
+    est2 = basic.output(plane=2)
+    assert np.abs(basic.plane_array(2) - est2).max() <= TYPICAL_TOL
+    final = vsfeel.BM3Dv2(clip, ref=basic, planes=[2], **PLANE_ARGS)
+    expected = oracle_lib.bm3d(clip.plane_array(2), _plane_params(2), ref=basic.plane_array(2))
+    assert np.abs(final.output(plane=2).astype(np.float64) - expected).max() <= OUT_TOL

@@ -1,0 +1,74 @@
+"""The wheel: builds offline from a copy of the tree, carries the package,
+the sm_100a library and the C header, is tagged py3-none-<platform>, and
+imports and loads the library once installed (CPU only; no kernel runs)."""
+
+from __future__ import annotations
+
+import shutil
+import subprocess
+import sys
+import zipfile
+
+import pytest
+
+from conftest import ROOT
+
+PKG_FILES = ("vsfeel/__init__.py", "vsfeel/_lib.py", "vsfeel/autograd.py", "vsfeel/batch.py",
+             "vsfeel/shard.py", "vsfeel/synthetic.py", "vsfeel/libvsfeel_bm3d.so",
+             "vsfeel/include/vsfeel_bm3d.h")
+
+
+@pytest.fixture(scope="module")
+def wheel(tmp_path_factory):
+    lib = ROOT / "vapoursynth-feel_b200" / "vsfeel" / "libvsfeel_bm3d.so"
+    if not lib.exists():
+        pytest.skip("library not built")
+    src = tmp_path_factory.mktemp("src")
+    for name in ("pyproject.toml", "setup.py", "README.md"):
+        shutil.copy2(ROOT / name, src / name)
+    shutil.copytree(ROOT / "include", src / "include")
+    # copy2 keeps the times, so the build reuses the library instead of recompiling
+    shutil.copytree(ROOT / "vapoursynth-feel_b200", src / "vapoursynth-feel_b200",
+                    ignore=shutil.ignore_patterns("__pycache__", "*.o"))
+    out = tmp_path_factory.mktemp("dist")
+    subprocess.run([sys.executable, "-m", "pip", "wheel", "--no-deps", "--no-build-isolation",
+                    "--no-index", "-q", "-w", str(out), str(src)], check=True, timeout=600)
+    wheels = list(out.glob("*.whl"))
+    assert len(wheels) == 1, wheels
+    return wheels[0]
+
+
+def test_wheel_contents_and_tag(wheel):
+    assert wheel.name.startswith("vapoursynth_feel_b200-1.0.0-py3-none-linux_")
+    with zipfile.ZipFile(wheel) as z:
+        names = set(z.namelist())
+        for f in PKG_FILES:
+            assert f in names, f
+        assert not any(n.startswith(("oracle/", "tests/", "csrc/")) for n in names)
+        info = next(n for n in names if n.endswith(".dist-info/WHEEL"))
+        text = z.read(info).decode()
+        assert "Root-Is-Purelib: false" in text
+        header = z.read("vsfeel/include/vsfeel_bm3d.h")
+    assert header == (ROOT / "include" / "vsfeel_bm3d.h").read_bytes()
+
+
+def test_installed_wheel_loads_the_library(wheel, tmp_path):
+    target = tmp_path / "site"
+    subprocess.run([sys.executable, "-m", "pip", "install", "--no-deps", "--no-index", "-q",
+                    "--target", str(target), str(wheel)], check=True, timeout=300)
+    code = (
+        "import sys; sys.path.insert(0, sys.argv[1]);"
+        "import vsfeel, os;"
+        "from vsfeel import _lib;"
+        "lib = _lib.load();"
+        "assert vsfeel.__file__.startswith(sys.argv[1]), vsfeel.__file__;"
+        "assert vsfeel.library_path().startswith(sys.argv[1]);"
+        "assert os.path.exists(os.path.join(vsfeel.get_include(), 'vsfeel_bm3d.h'));"
+        "assert vsfeel.get_include().startswith(sys.argv[1]);"
+        "print(lib.vsfeel_bm3d_abi_version())"
+    )
+    # run outside the checkout so that nothing resolves to the source tree
+    res = subprocess.run([sys.executable, "-c", code, str(target)], capture_output=True,
+                         text=True, cwd=tmp_path, timeout=120)
+    assert res.returncode == 0, res.stderr
+    assert res.stdout.strip() == "1"

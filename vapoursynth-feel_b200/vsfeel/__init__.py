@@ -28,7 +28,25 @@ import numpy as np
 from . import _lib
 
 __all__ = ["Error", "VideoFormat", "GRAYS", "YUV420PS", "YUV444PS", "VideoNode", "VideoFrame",
-           "clip_from_array", "BM3Dv2", "bm3d_device", "plane_params"]
+           "clip_from_array", "BM3Dv2", "bm3d_device", "plane_params", "get_include",
+           "library_path"]
+
+__version__ = "1.0.0"
+
+
+def get_include() -> str:
+    """The directory holding vsfeel_bm3d.h: inside an installed wheel, or the
+    checkout's include/ when the package runs from the source tree."""
+    from pathlib import Path
+
+    here = Path(__file__).resolve().parent
+    packaged = here / "include"
+    return str(packaged if (packaged / "vsfeel_bm3d.h").exists() else here.parent.parent / "include")
+
+
+def library_path() -> str:
+    """The C-ABI library (libvsfeel_bm3d.so) that other languages link or load."""
+    return str(_lib.LIB_PATH)
 
 
 class Error(Exception):
@@ -182,6 +200,7 @@ class BM3DNode(VideoNode):
         self._src = clip
         self._ctxs = {c.plane: c for c in ctxs}
         self._ctx = ctxs[0]
+        self._whole: dict[int, np.ndarray] = {}
         self._plane_src = {p: np.ascontiguousarray(clip.plane_array(p), dtype=np.float32)
                            for p in self._ctxs}
         # the final (Wiener) pass: the basic estimate that matching runs on
@@ -193,6 +212,17 @@ class BM3DNode(VideoNode):
     def planes(self) -> list[int]:
         """The denoised planes, in the order given."""
         return list(self._ctxs)
+
+    def plane_array(self, p: int = 0) -> np.ndarray:
+        """Plane p of every output frame, (N, h, w): denoised planes are
+        computed once on first use, the others are the source's. This makes
+        the node usable wherever a clip is, e.g. as ``ref`` of the final
+        pass."""
+        if p not in self._ctxs:
+            return self._src.plane_array(p)
+        if p not in self._whole:
+            self._whole[p] = self.output(plane=p)
+        return self._whole[p]
 
     @property
     def final_pass(self) -> bool:
