@@ -340,6 +340,33 @@ def time_all_planes(torch, dev, nfr, steps, warmup):
             "steps": steps, "warmup": warmup}
 
 
+def time_frame_requests(luma, u, v, dev_index, passes, threads):
+    """The VapourSynth request path as vspipe drives it: get_frame(n) for
+    n = 0..N-1 submitted in order to `threads` worker threads (that many
+    requests in flight, fmParallel), the frames fetched from pageable host
+    memory through the callbacks and each output copied back. Wall clock;
+    each pass denoises the whole clip (the stack cache is smaller than the
+    clip, so a pass recomputes every stack)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import vsfeel
+
+    node = vsfeel.BM3Dv2(vsfeel.clip_from_array(luma, u, v), device=dev_index, **PARAMS)
+    n = luma.shape[0]
+    node.get_frame(0)
+    launches0 = node.launch_count()
+    with ThreadPoolExecutor(threads) as ex:
+        t0 = time.perf_counter()
+        for _ in range(passes):
+            list(ex.map(node.get_frame, range(n)))
+        sec = (time.perf_counter() - t0) / passes
+    return {"workload": f"bm3dv2_get_frame_in_order_yuv420ps_1920x1080x{n}_r2",
+            "threads": threads, "mpx_s": n * luma.shape[1] * luma.shape[2] / sec / 1e6,
+            "ms_per_clip": sec * 1e3,
+            "launches_per_frame": (node.launch_count() - launches0) / (passes * n),
+            "passes": passes}
+
+
 def run_reference(args) -> int:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -547,6 +574,9 @@ def main() -> int:
                            for name in GRAD_WORKLOADS]
     if world == 1 and not args.no_batch:
         line["batched"] = time_batched(torch, dev, max(2, args.steps // 3), 3)
+    if world == 1 and not args.no_e2e:
+        line["frame_requests"] = [time_frame_requests(luma, u, v, local_rank, 2, t)
+                                  for t in (1, 4)]
     if world == 1 and not args.no_planes:
         line["all_planes"] = time_all_planes(torch, dev, nfr, max(3, args.steps // 2), 3)
     if world == 1 and not args.no_cpu_baseline:

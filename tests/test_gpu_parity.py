@@ -142,6 +142,51 @@ def test_get_frame_matches_whole_clip():
         assert np.abs(f[0] - whole[n]).max() <= TYPICAL_TOL, n
 
 
+@pytest.mark.parametrize("order", [
+    list(range(12)),                                  # in order
+    [2, 0, 3, 1, 6, 4, 5, 7, 10, 8, 11, 9],           # four requests in flight
+])
+def test_get_frame_computes_each_stack_once(order):
+    """The request path caches whole stacks (the reference's result cache,
+    src/bm3d.cpp:380-478): in order, or out of order within the cache, every
+    stack is matched and filtered once and every request normalises once."""
+    frames = make_clip(12, 64, 80, sigma=5.0, seed=21)
+    node = _node(frames, sigma=5.0, block_step=4, bm_range=10, radius=2, ps_num=2, ps_range=4)
+    whole = node.output()
+    l0 = node.launch_count()
+    for n in order:
+        assert np.abs(node.get_frame(n)[0] - whole[n]).max() <= TYPICAL_TOL, n
+    assert node.launch_count() - l0 == 12 * 2 + 12
+    # a request far behind recomputes only the stacks it misses, correctly
+    l1 = node.launch_count()
+    assert np.abs(node.get_frame(0)[0] - whole[0]).max() <= TYPICAL_TOL
+    assert node.launch_count() - l1 == 3 * 2 + 1
+
+
+def test_get_frame_stack_cache_at_clip_ends_and_radius_zero():
+    for r, n in ((0, 5), (1, 2), (3, 7), (4, 9)):
+        frames = make_clip(n, 40, 48, sigma=4.0, seed=30 + r)
+        node = _node(frames, sigma=4.0, block_step=3, bm_range=6, radius=r, ps_num=2, ps_range=3)
+        whole = node.output()
+        for k in list(range(n - 1, -1, -1)) + [n // 2]:
+            assert np.abs(node.get_frame(k)[0] - whole[k]).max() <= TYPICAL_TOL, (r, k)
+
+
+def test_concurrent_requests_match_whole_clip():
+    """fmParallel: requests from more threads than request slots, in and out
+    of order; every output equals the whole-clip result."""
+    from concurrent.futures import ThreadPoolExecutor
+    frames = make_clip(16, 64, 80, sigma=5.0, seed=22)
+    node = _node(frames, sigma=5.0, block_step=4, bm_range=10, radius=2, ps_num=2, ps_range=4,
+                 num_streams=2)
+    whole = node.output()
+    order = list(range(16)) + [3, 15, 0, 9]
+    with ThreadPoolExecutor(6) as ex:
+        outs = list(ex.map(lambda k: node.get_frame(k)[0], order))
+    for k, o in zip(order, outs):
+        assert np.abs(o - whole[k]).max() <= TYPICAL_TOL, k
+
+
 def test_frame_range_mirrors_request_window():
     node = _node(make_clip(10, 16, 16, seed=1), radius=2)
     assert node.frame_range(0) == (0, 4)

@@ -26,11 +26,13 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <condition_variable>
 #include <functional>
 #include <map>
 #include <mutex>
 #include <string>
 #include <thread>
+#include <type_traits>
 #include <vector>
 
 namespace {
@@ -76,6 +78,25 @@ int64_t timeout_ms() {
         if (v > 0) return v;
     }
     return 120000;
+}
+
+// Bounded wait on an event: polls until it has fired or the deadline passes.
+int wait_event(cudaEvent_t e, int64_t limit_ms) {
+    const auto t0 = std::chrono::steady_clock::now();
+    int spins = 0;
+    for (;;) {
+        const cudaError_t q = cudaEventQuery(e);
+        if (q == cudaSuccess) return VSFEEL_OK;
+        if (q != cudaErrorNotReady)
+            return fail(VSFEEL_E_CUDA, std::string("CUDA error: ") + cudaGetErrorString(q));
+        const auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(
+                            std::chrono::steady_clock::now() - t0)
+                            .count();
+        if (ms >= limit_ms)
+            return fail(VSFEEL_E_TIMEOUT, "timed out after " + std::to_string(ms) +
+                                              " ms waiting for the GPU");
+        if (++spins > 64) std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
 }
 
 // Bounded wait on a stream: polls until idle or the deadline passes.
@@ -284,13 +305,15 @@ struct vsfeel_bm3d {
     // context's buffers.
     cudaEvent_t tail = nullptr;
     bool tail_set = false;
+    bool tail_from_request = false;  // set by the per-frame path, which orders its own work
     void after_prior(cudaStream_t st) {
         if (tail_set) VSF_CUDA(cudaStreamWaitEvent(st, tail, 0));
     }
-    void mark_tail(cudaStream_t st) {
+    void mark_tail(cudaStream_t st, bool from_request = false) {
         if (!tail) VSF_CUDA(cudaEventCreateWithFlags(&tail, cudaEventDisableTiming));
         VSF_CUDA(cudaEventRecord(tail, st));
         tail_set = true;
+        tail_from_request = from_request;
     }
 
     void copy_streams(size_t nframes_in, size_t nout) {
@@ -329,6 +352,70 @@ struct vsfeel_bm3d {
     }
     std::map<int, int> frame_slot;  // frame cache of the per-frame path
     std::vector<int> slot_frame;
+    // Stack cache of the per-frame path: slot c holds the TW (numerator,
+    // weight) slice pairs of stack stack_tag[c] (-1: empty), last used at
+    // request stack_use[c].
+    DevBuf<float> stackcache;
+    std::vector<int> stack_tag;
+    std::vector<int64_t> stack_use;
+    int64_t requests = 0;
+    int stack_slots() const { return tw() + std::min(s.num_streams, 16); }
+    float* stack_slices(int c) { return stackcache.p + (size_t)c * tw() * 2 * acc_plane; }
+
+    // Page-locked staging of the per-frame path, so that requests from
+    // several threads overlap their host copies with each other's kernels.
+    // Uploads: a fetched frame is copied on the host into one of kUpSlots
+    // page-locked planes and released at once; the plane is reused after
+    // its device copy has run (up_done). Outputs: each request holds a
+    // request slot (device plane, page-locked plane and status word, event)
+    // from enqueue until its caller has copied the output out.
+    static constexpr int kUpSlots = 8;
+    float* up_host = nullptr;
+    cudaEvent_t up_done[kUpSlots] = {};
+    bool up_used[kUpSlots] = {};
+    int up_next = 0;
+    struct RequestSlot {
+        float* dev = nullptr;
+        float* host = nullptr;
+        int* status = nullptr;
+        cudaEvent_t normalised = nullptr, done = nullptr;
+        bool busy = false;
+    };
+    // per frame-cache slot: recorded after the last stack that read it, so
+    // that an upload into the slot on the copy stream waits for that stack
+    std::vector<cudaEvent_t> frame_read;
+    std::vector<char> frame_read_set;
+    std::vector<RequestSlot> req_slots;
+    unsigned char* req_host = nullptr;
+    DevBuf<float> req_dev;
+    std::condition_variable req_cv;
+    std::atomic<int> requests_in_flight{0};  // callers inside get_frame
+    int request_slots() const { return std::max(2, std::min(s.num_streams, 16)); }
+    size_t packed_plane_floats() const { return (size_t)s.width * s.height; }
+    void request_staging() {
+        if (!up_host) {
+            VSF_CUDA(cudaHostAlloc(&up_host, sizeof(float) * packed_plane_floats() * kUpSlots,
+                                   cudaHostAllocPortable));
+            for (auto& e : up_done) VSF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        }
+        if (req_slots.empty()) {
+            const int k = request_slots();
+            const size_t host_bytes = sizeof(float) * packed_plane_floats() + 64;
+            VSF_CUDA(cudaHostAlloc(&req_host, host_bytes * k, cudaHostAllocPortable));
+            req_dev.ensure(frame_floats() * k);
+            req_slots.resize(k);
+            for (int i = 0; i < k; ++i) {
+                RequestSlot& r = req_slots[i];
+                r.dev = req_dev.p + frame_floats() * i;
+                r.host = reinterpret_cast<float*>(req_host + host_bytes * i);
+                r.status = reinterpret_cast<int*>(req_host + host_bytes * i +
+                                                  sizeof(float) * packed_plane_floats());
+                VSF_CUDA(cudaEventCreateWithFlags(&r.normalised, cudaEventDisableTiming));
+                VSF_CUDA(cudaEventCreateWithFlags(&r.done, cudaEventDisableTiming));
+            }
+        }
+        copy_streams(0, 0);
+    }
 
     // event trace: (kind, start, stop) per traced launch
     struct Mark {
@@ -404,7 +491,8 @@ struct vsfeel_bm3d {
     void launch_stack(int m, const std::function<const float*(int)>& frame_ptr, int in_pitch,
                       int out_lo, int out_hi, cudaStream_t st, unsigned char* saved = nullptr,
                       bool table_only = false,
-                      const std::function<const float*(int)>* input_ptr = nullptr) {
+                      const std::function<const float*(int)>* input_ptr = nullptr,
+                      float* own_slices = nullptr) {
         const int r = s.radius;
         StackJob job{};
         for (int z = 0; z < tw(); ++z) {
@@ -412,8 +500,11 @@ struct vsfeel_bm3d {
             job.slice_input[z] = input_ptr ? (*input_ptr)(clampf(m - r + z)) : nullptr;
             const int n = clampf(m - r + z);
             job.slice_dst[z] = nullptr;
+            // slice z goes to the output that reads it: into that output's
+            // ring slot, or (own_slices) into the stack's own slice z
             if (n >= out_lo && n <= out_hi && read_slice(n, m) == z)
-                job.slice_dst[z] = slot_pair(n, m - (n - r));
+                job.slice_dst[z] = own_slices ? own_slices + (size_t)z * 2 * acc_plane
+                                              : slot_pair(n, m - (n - r));
         }
         job.dst_plane = (int64_t)acc_plane;
         job.pitch = in_pitch;
@@ -461,13 +552,18 @@ struct vsfeel_bm3d {
         launches += 2;
     }
 
+    // stack_slices_of(m): stack m's own slices (the stack cache); by default
+    // output n's ring slot
     void launch_normalize(int n, float* out, int out_pitch, cudaStream_t st,
-                          unsigned char* saved = nullptr) {
+                          unsigned char* saved = nullptr,
+                          const std::function<float*(int)>* stack_slices_of = nullptr) {
         const int r = s.radius;
         NormalizeJob job{};
         for (int i = 0; i < tw(); ++i) {
             const int m = clampf(n - r + i);
-            job.num[i] = slot_pair(n, m - (n - r));
+            job.num[i] = stack_slices_of
+                             ? (*stack_slices_of)(m) + (size_t)read_slice(n, m) * 2 * acc_plane
+                             : slot_pair(n, m - (n - r));
         }
         job.den_offset = (int64_t)acc_plane;
         job.tw = tw();
@@ -529,10 +625,13 @@ namespace {
 template <class F>
 int guarded(vsfeel_bm3d* ctx, F&& fn) {
     if (!ctx) return fail(VSFEEL_E_ARG, "null context");
-    std::lock_guard<std::mutex> lk(ctx->lock);
+    std::unique_lock<std::mutex> lk(ctx->lock);
     DeviceGuard dg(ctx->device);
     try {
-        return fn();
+        if constexpr (std::is_invocable_v<F, std::unique_lock<std::mutex>&>)
+            return fn(lk);
+        else
+            return fn();
     } catch (const CudaError& e) {
         if (e.err == cudaErrorMemoryAllocation) {
             cudaGetLastError();
@@ -658,6 +757,17 @@ void vsfeel_bm3d_free(vsfeel_bm3d* ctx) {
         ctx->match_z.release();
         ctx->frames.release();
         ctx->outbuf.release();
+        ctx->stackcache.release();
+        for (int i = 0; i < vsfeel_bm3d::kUpSlots; ++i)
+            if (ctx->up_done[i]) cudaEventDestroy(ctx->up_done[i]);
+        if (ctx->up_host) cudaFreeHost(ctx->up_host);
+        for (auto& r : ctx->req_slots) {
+            if (r.normalised) cudaEventDestroy(r.normalised);
+            if (r.done) cudaEventDestroy(r.done);
+        }
+        for (cudaEvent_t e : ctx->frame_read) cudaEventDestroy(e);
+        if (ctx->req_host) cudaFreeHost(ctx->req_host);
+        ctx->req_dev.release();
         ctx->status.release();
         for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     }
@@ -690,7 +800,7 @@ int vsfeel_bm3d_get_info(const vsfeel_bm3d* ctx, vsfeel_bm3d_info* info) {
     info->extractor = s.extractor;
     info->blocks_x = ctx->nbx;
     info->blocks_y = ctx->nby;
-    info->device_bytes = (int64_t)(ctx->ring.n + ctx->frames.n + ctx->outbuf.n) * 4 +
+    info->device_bytes = (int64_t)(ctx->ring.n + ctx->frames.n + ctx->outbuf.n + ctx->stackcache.n) * 4 +
                          (int64_t)(ctx->match_xy.n + ctx->match_z.n) * 4;
     return VSFEEL_OK;
 }
@@ -899,12 +1009,47 @@ int process_host(vsfeel_bm3d* ctx, const float* src, ptrdiff_t src_frame_stride_
 
 // The per-frame request path. fetch(clip, f, &stride) returns frame f of
 // the source (clip 0) or the ref clip (1); release(clip, f) hands it back.
-// A cache slot holds a frame's source plane and, in the final pass, its ref
-// plane after it.
+// A frame-cache slot holds a frame's source plane and, in the final pass,
+// its ref plane after it.
+//
+// Stacks are cached whole, as the reference's result cache holds them
+// (src/bm3d.cpp:380-478): a stack writes each slice that an output reads
+// into its own cache slot, and output n is normalised from slice
+// agg_z(i, n) of the cached stacks clamp(n - r + i). Requests in any order
+// compute a stack once while it stays among the stack_slots() most recently
+// used; a request computes only the stacks it misses, fetching frames of
+// its frame_range window only.
+//
+// When other requests are in flight, a request holds the context's lock
+// only while it enqueues: frames are copied into page-locked staging on the
+// host and released at once, the output comes back into the request's
+// page-locked slot, and the caller waits for its own event and copies the
+// rows out with the lock released. Requests from several threads
+// (fmParallel) thus overlap their host copies with each other's kernels;
+// the GPU work stays in request order on the context's stream. A request
+// alone in flight copies straight from and to the caller's memory instead
+// (the driver pipelines pageable copies faster than a host copy plus DMA).
 int get_frame(vsfeel_bm3d* ctx, int n, bool with_ref,
               const std::function<const float*(int, int, ptrdiff_t*)>& fetch,
               const std::function<void(int, int)>& release, float* dst, ptrdiff_t dst_stride_bytes) {
-    return guarded(ctx, [&]() -> int {
+    if (!ctx) return fail(VSFEEL_E_ARG, "null context");
+    // counted before the lock, so that callers waiting for it count too
+    struct InFlight {
+        std::atomic<int>& c;
+        explicit InFlight(std::atomic<int>& c_) : c(c_) { ++c; }
+        ~InFlight() { --c; }
+    } in_flight(ctx->requests_in_flight);
+    int slot = -1;
+    bool direct = false;  // alone in flight: copies from and to the caller's memory
+    auto hand_back = [&] {
+        if (slot < 0) return;
+        {
+            std::lock_guard<std::mutex> lk(ctx->lock);
+            ctx->req_slots[slot].busy = false;
+        }
+        ctx->req_cv.notify_one();
+    };
+    int rc = guarded(ctx, [&](std::unique_lock<std::mutex>& lk) -> int {
         const Settings& s = ctx->s;
         int rc = check_pass(ctx, with_ref);
         if (rc != VSFEEL_OK) return rc;
@@ -913,20 +1058,55 @@ int get_frame(vsfeel_bm3d* ctx, int n, bool with_ref,
         const size_t row_bytes = sizeof(float) * (size_t)s.width;
         if (dst_stride_bytes < (ptrdiff_t)row_bytes)
             return fail(VSFEEL_E_ARG, "row stride smaller than the width");
+        ctx->request_staging();
+        // a free request slot; others are handed back as their callers finish
+        auto free_slot = [&] {
+            for (size_t i = 0; i < ctx->req_slots.size(); ++i)
+                if (!ctx->req_slots[i].busy) return (int)i;
+            return -1;
+        };
+        if (!ctx->req_cv.wait_for(lk, std::chrono::milliseconds(timeout_ms()),
+                                  [&] { return free_slot() >= 0; }))
+            return fail(VSFEEL_E_TIMEOUT, "timed out waiting for a request slot");
+        slot = free_slot();
+        ctx->req_slots[slot].busy = true;
+        direct = ctx->requests_in_flight.load() == 1;
+
         const int r = s.radius;
         const int planes = with_ref ? 2 : 1;
         const int f_lo = ctx->clampf(n - 2 * r), f_hi = ctx->clampf(n + 2 * r);
         const int cap = 4 * r + 2;  // window plus one frame of slack
+        const int nstack = ctx->stack_slots();
         const size_t ff = ctx->frame_floats();
+        const size_t pf = ctx->packed_plane_floats();
         if ((int)ctx->slot_frame.size() != cap) {
             ctx->frame_slot.clear();
             ctx->slot_frame.assign(cap, -1);
         }
+        while ((int)ctx->frame_read.size() < cap) {
+            cudaEvent_t e;
+            VSF_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            ctx->frame_read.push_back(e);
+            ctx->frame_read_set.push_back(0);
+        }
+        if ((int)ctx->stack_tag.size() != nstack) {
+            ctx->stack_tag.assign(nstack, -1);
+            ctx->stack_use.assign(nstack, -1);
+        }
         ctx->frames.ensure(ff * cap * planes);
-        ctx->outbuf.ensure(ff);
+        ctx->stackcache.ensure((size_t)nstack * ctx->tw() * 2 * ctx->acc_plane);
+        ctx->match_xy.ensure((size_t)ctx->nblocks * 8);
+        ctx->match_z.ensure((size_t)ctx->nblocks);
+        const int64_t req = ++ctx->requests;
         cudaStream_t st = ctx->stream;
-        ctx->after_prior(st);
-        // evict cached frames outside the window, then upload the missing ones
+        // another entry point's work first; the per-frame path's own work is
+        // ordered by the events below
+        if (!ctx->tail_from_request) {
+            ctx->after_prior(st);
+            ctx->after_prior(ctx->up_stream);
+            ctx->after_prior(ctx->down_stream);
+        }
+        // evict cached frames outside the window
         for (auto it = ctx->frame_slot.begin(); it != ctx->frame_slot.end();) {
             if (it->first < f_lo || it->first > f_hi) {
                 ctx->slot_frame[it->second] = -1;
@@ -935,49 +1115,166 @@ int get_frame(vsfeel_bm3d* ctx, int n, bool with_ref,
                 ++it;
             }
         }
-        for (int f = f_lo; f <= f_hi; ++f) {
-            if (ctx->frame_slot.count(f)) continue;
-            int slot = 0;
-            while (ctx->slot_frame[slot] != -1) ++slot;
-            for (int clip = 0; clip < planes; ++clip) {
-                ptrdiff_t stride = 0;
-                const float* p = fetch(clip, f, &stride);
-                if (!p)
-                    return fail(VSFEEL_E_FETCH, std::string("could not fetch ") +
-                                                    (clip ? "\"ref\" frame " : "source frame ") +
-                                                    std::to_string(f));
-                if (stride < (ptrdiff_t)row_bytes) {
+        // frames lo..hi resident (all inside the window)
+        auto stage = [&](int lo, int hi) -> int {
+            for (int f = lo; f <= hi; ++f) {
+                if (ctx->frame_slot.count(f)) continue;
+                int slot_f = 0;
+                while (ctx->slot_frame[slot_f] != -1) ++slot_f;
+                for (int clip = 0; clip < planes; ++clip) {
+                    if (direct) {
+                        ptrdiff_t stride = 0;
+                        const float* p = fetch(clip, f, &stride);
+                        if (!p)
+                            return fail(VSFEEL_E_FETCH,
+                                        std::string("could not fetch ") +
+                                            (clip ? "\"ref\" frame " : "source frame ") +
+                                            std::to_string(f));
+                        if (stride < (ptrdiff_t)row_bytes) {
+                            release(clip, f);
+                            return fail(VSFEEL_E_ARG, "source row stride smaller than the width");
+                        }
+                        VSF_CUDA(cudaMemcpy2DAsync(
+                            ctx->frames.p + ((size_t)slot_f * planes + clip) * ff,
+                            sizeof(float) * ctx->acc_pitch, p, stride, row_bytes, s.height,
+                            cudaMemcpyHostToDevice, st));
+                        // the source frame must stay valid until the copy has run
+                        const int wrc = wait_stream(st, timeout_ms());
+                        release(clip, f);
+                        if (wrc != VSFEEL_OK) return wrc;
+                        continue;
+                    }
+                    const int k = ctx->up_next;
+                    ctx->up_next = (k + 1) % vsfeel_bm3d::kUpSlots;
+                    if (ctx->up_used[k]) {
+                        const int wrc = wait_event(ctx->up_done[k], timeout_ms());
+                        if (wrc != VSFEEL_OK) return wrc;
+                    }
+                    ptrdiff_t stride = 0;
+                    const float* p = fetch(clip, f, &stride);
+                    if (!p)
+                        return fail(VSFEEL_E_FETCH, std::string("could not fetch ") +
+                                                        (clip ? "\"ref\" frame " : "source frame ") +
+                                                        std::to_string(f));
+                    if (stride < (ptrdiff_t)row_bytes) {
+                        release(clip, f);
+                        return fail(VSFEEL_E_ARG, "source row stride smaller than the width");
+                    }
+                    float* staged = ctx->up_host + pf * k;
+                    const unsigned char* row = reinterpret_cast<const unsigned char*>(p);
+                    for (int y = 0; y < s.height; ++y)
+                        std::memcpy(staged + (size_t)y * s.width, row + (size_t)y * stride, row_bytes);
                     release(clip, f);
-                    return fail(VSFEEL_E_ARG, "source row stride smaller than the width");
+                    // on the copy stream, after the last stack that read the
+                    // slot's previous frame; the stacks wait for the copy
+                    cudaStream_t up = ctx->up_stream;
+                    if (ctx->frame_read_set[slot_f])
+                        VSF_CUDA(cudaStreamWaitEvent(up, ctx->frame_read[slot_f], 0));
+                    VSF_CUDA(cudaMemcpy2DAsync(ctx->frames.p + ((size_t)slot_f * planes + clip) * ff,
+                                               sizeof(float) * ctx->acc_pitch, staged, row_bytes,
+                                               row_bytes, s.height, cudaMemcpyHostToDevice, up));
+                    VSF_CUDA(cudaEventRecord(ctx->up_done[k], up));
+                    VSF_CUDA(cudaStreamWaitEvent(st, ctx->up_done[k], 0));
+                    ctx->up_used[k] = true;
                 }
-                VSF_CUDA(cudaMemcpy2DAsync(ctx->frames.p + ((size_t)slot * planes + clip) * ff,
-                                           sizeof(float) * ctx->acc_pitch, p, stride, row_bytes,
-                                           s.height, cudaMemcpyHostToDevice, st));
-                // the source frame must stay valid until the copy has run
-                const int wrc = wait_stream(st, timeout_ms());
-                release(clip, f);
-                if (wrc != VSFEEL_OK) return wrc;
+                ctx->slot_frame[slot_f] = f;
+                ctx->frame_slot[f] = slot_f;
             }
-            ctx->slot_frame[slot] = f;
-            ctx->frame_slot[f] = slot;
-        }
+            return VSFEEL_OK;
+        };
         auto plane_at = [&](int f, int clip) -> const float* {
             return ctx->frames.p + ((size_t)ctx->frame_slot.at(f) * planes + clip) * ff;
         };
-        auto out_at = [&](int) { return ctx->outbuf.p; };
-        if (!with_ref) {
-            ctx->run([&](int f) { return plane_at(f, 0); }, ctx->acc_pitch, out_at, ctx->acc_pitch,
-                     n, 1, st);
-        } else {
-            const std::function<const float*(int)> input = [&](int f) { return plane_at(f, 0); };
-            ctx->run([&](int f) { return plane_at(f, 1); }, ctx->acc_pitch, out_at, ctx->acc_pitch,
-                     n, 1, st, nullptr, &input);
+        const std::function<const float*(int)> search = [&](int f) {
+            return plane_at(f, with_ref ? 1 : 0);
+        };
+        const std::function<const float*(int)> input = [&](int f) { return plane_at(f, 0); };
+        auto slot_of = [&](int m) {
+            for (int c = 0; c < nstack; ++c)
+                if (ctx->stack_tag[c] == m) return c;
+            return -1;
+        };
+
+        // the stacks output n reads, each pinned for this request
+        const int m_lo = ctx->clampf(n - r), m_hi = ctx->clampf(n + r);
+        for (int m = m_lo; m <= m_hi; ++m) {
+            const int c = slot_of(m);
+            if (c >= 0) ctx->stack_use[c] = req;
         }
-        VSF_CUDA(cudaMemcpy2DAsync(dst, dst_stride_bytes, ctx->outbuf.p, sizeof(float) * ctx->acc_pitch,
-                                   row_bytes, s.height, cudaMemcpyDeviceToHost, st));
-        ctx->mark_tail(st);
-        return ctx->finish(st);
+        for (int m = m_lo; m <= m_hi; ++m) {
+            if (slot_of(m) >= 0) continue;
+            // least recently used slot not pinned by this request (the
+            // cache holds more than 2r+1 stacks, so one exists)
+            int c = -1;
+            for (int k = 0; k < nstack; ++k)
+                if (ctx->stack_use[k] != req && (c < 0 || ctx->stack_use[k] < ctx->stack_use[c]))
+                    c = k;
+            ctx->stack_tag[c] = -1;
+            rc = stage(ctx->clampf(m - r), ctx->clampf(m + r));
+            if (rc != VSFEEL_OK) return rc;
+            float* slices = ctx->stack_slices(c);
+            VSF_CUDA(cudaMemsetAsync(slices, 0, sizeof(float) * (size_t)ctx->tw() * 2 * ctx->acc_plane,
+                                     st));
+            ctx->launch_stack(m, search, ctx->acc_pitch, 0, s.nframes - 1, st, nullptr, false,
+                              with_ref ? &input : nullptr, slices);
+            for (int f = ctx->clampf(m - r); f <= ctx->clampf(m + r); ++f) {
+                const int fs = ctx->frame_slot.at(f);
+                VSF_CUDA(cudaEventRecord(ctx->frame_read[fs], st));
+                ctx->frame_read_set[fs] = 1;
+            }
+            ctx->stack_tag[c] = m;
+            ctx->stack_use[c] = req;
+        }
+        const std::function<float*(int)> slices_of = [&](int m) {
+            return ctx->stack_slices(slot_of(m));
+        };
+        vsfeel_bm3d::RequestSlot& rs = ctx->req_slots[slot];
+        ctx->launch_normalize(n, rs.dev, ctx->acc_pitch, st, nullptr, &slices_of);
+        if (direct) {
+            VSF_CUDA(cudaMemcpy2DAsync(dst, dst_stride_bytes, rs.dev, sizeof(float) * ctx->acc_pitch,
+                                       row_bytes, s.height, cudaMemcpyDeviceToHost, st));
+            ctx->mark_tail(st, true);
+            return ctx->finish(st);
+        }
+        // the download on the other copy stream, after the normalisation
+        cudaStream_t down = ctx->down_stream;
+        int* status = ctx->status_word();
+        VSF_CUDA(cudaEventRecord(rs.normalised, st));
+        VSF_CUDA(cudaStreamWaitEvent(down, rs.normalised, 0));
+        VSF_CUDA(cudaMemcpy2DAsync(rs.host, row_bytes, rs.dev, sizeof(float) * ctx->acc_pitch,
+                                   row_bytes, s.height, cudaMemcpyDeviceToHost, down));
+        VSF_CUDA(cudaMemcpyAsync(rs.status, status, sizeof(int), cudaMemcpyDeviceToHost, down));
+        VSF_CUDA(cudaEventRecord(rs.done, down));
+        // the download stream has waited for everything this request put on
+        // the compute stream, so its end is the end of the request
+        ctx->mark_tail(down, true);
+        return VSFEEL_OK;
     });
+    if (rc != VSFEEL_OK || direct) {
+        hand_back();
+        return rc;
+    }
+    // the caller's wait and copy, with the lock released
+    const vsfeel_bm3d::RequestSlot& rs = ctx->req_slots[slot];
+    {
+        DeviceGuard dg(ctx->device);
+        rc = wait_event(rs.done, timeout_ms());
+    }
+    if (rc == VSFEEL_OK && *rs.status != 0) {
+        rc = guarded(ctx, [&]() -> int {
+            VSF_CUDA(cudaMemsetAsync(ctx->status.p, 0, sizeof(int), ctx->stream));
+            return fail(VSFEEL_E_CUDA, "internal error: a search window left the staged region");
+        });
+    }
+    if (rc == VSFEEL_OK) {
+        const size_t row_bytes = sizeof(float) * (size_t)ctx->s.width;
+        unsigned char* out = reinterpret_cast<unsigned char*>(dst);
+        for (int y = 0; y < ctx->s.height; ++y)
+            std::memcpy(out + (size_t)y * dst_stride_bytes, rs.host + (size_t)y * ctx->s.width,
+                        row_bytes);
+    }
+    hand_back();
+    return rc;
 }
 
 }  // namespace
