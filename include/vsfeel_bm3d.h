@@ -123,7 +123,11 @@ typedef const float* (*vsfeel_fetch_fn)(void* user, int n, ptrdiff_t* stride_byt
 typedef void (*vsfeel_release_fn)(void* user, int n);
 
 /* arAllFramesReady: denoises output frame n into dst (luma plane). Frames
- * are fetched through the callbacks only when not already resident. */
+ * are fetched through the callbacks only when not already resident (the
+ * frames of frame_range(n) only), and computed stacks are cached, so
+ * requests in or near order compute each stack once. Calls from several
+ * threads may overlap: a call holds the context while it enqueues its work
+ * and waits for its own output without it. */
 VSFEEL_API int vsfeel_bm3d_get_frame(vsfeel_bm3d* ctx, int n, vsfeel_fetch_fn fetch,
                           vsfeel_release_fn release, void* user, float* dst,
                           ptrdiff_t dst_stride_bytes);
