@@ -16,7 +16,8 @@
  * returns 0 on success or a negative VSFEEL_E_* code; the message (prefixed
  * "BM3D: " like the reference's errors) is available from
  * vsfeel_bm3d_last_error() on the calling thread. A context is internally
- * synchronised: calls from several threads are serialised. Strides are in
+ * synchronised: calls from several threads are serialised (get_frame calls
+ * only while they enqueue their work). Strides are in
  * bytes for host buffers and in elements (floats) for device buffers.
  */
 #ifndef VSFEEL_BM3D_H
@@ -64,7 +65,8 @@ typedef struct vsfeel_bm3d_video_info {
 /* The BM3Dv2 argument map (registration string at src/bm3d.cpp:1562-1571).
  * An array argument with count 0 is absent and takes the reference default;
  * a missing element copies the previous one (src/bm3d.cpp:1090-1167).
- * Only element [0] of each array is used, as in the reference. */
+ * Only element [0] of each array is used, as in the reference, except by
+ * vsfeel_bm3d_create_plane for planes 1 and 2. */
 typedef struct vsfeel_bm3d_args {
     float sigma[3];      int sigma_count;       /* default 3.0  */
     int block_step[3];   int block_step_count;  /* default 8    */
