@@ -637,7 +637,11 @@ __device__ __forceinline__ uint32_t key_xy(uint64_t key, const Window* wins, int
 
 // Stages frame rows [ry0, ry1] x columns [rx0, rx1] into smem, column-major
 // with column stride cs (odd, so the transposing stores of a warp hit
-// distinct banks). Global reads are coalesced along rows.
+// distinct banks). Global reads are coalesced along rows. The copies are
+// asynchronous (cp.async, 4 bytes each): a thread issues all of its copies
+// before waiting once, so the L2 latency of the region is paid about once
+// rather than once per dependent load and store. The caller synchronises
+// the CTA afterwards.
 __device__ void stage_region(float* smem, const float* __restrict__ frame, int pitch, int rx0,
                              int ry0, int rx1, int ry1, int cs) {
     const int w = rx1 - rx0 + 1;
@@ -645,8 +649,13 @@ __device__ void stage_region(float* smem, const float* __restrict__ frame, int p
     const int lane = threadIdx.x & 31;
     for (int yy = threadIdx.x >> 5; yy < h; yy += blockDim.x >> 5) {
         const float* __restrict__ row = frame + (size_t)(ry0 + yy) * pitch + rx0;
-        for (int xx = lane; xx < w; xx += 32) smem[xx * cs + yy] = __ldg(row + xx);
+        for (int xx = lane; xx < w; xx += 32) {
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(smem + xx * cs + yy);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(row + xx)
+                         : "memory");
+        }
     }
+    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 struct SmemPlan {
