@@ -237,8 +237,8 @@ __device__ __forceinline__ void scan_chunk(const Region& reg, const float* cur_s
 // reference's operands: P01(j-1) = S0(j-1) + S1(j), P23(j-3) = S2(j-1) +
 // S3(j), P45(j-5) = S4(j-1) + S5(j), P67(j-7) = S6(j-1) + S7(j),
 // Q0123(j-3) = P01(j-3) + P23(j-3), Q4567(j-7) = P45(j-7) + P67(j-7),
-// E(j-7) = Q0123(j-7) + Q4567(j-7). Each block column is read from shared
-// memory once per step and used for all K rows. With 136 flops per candidate
+// E(j-7) = Q0123(j-7) + Q4567(j-7). The block is read from shared memory
+// once per step and used for all K rows. With 136 flops per candidate
 // the selection is cheap next to the scan, so there is no error table: each
 // candidate's (error, scan index) key goes straight into the lane's sorted
 // top-8 (top, ascending), and the 8 lane lists are merged afterwards.
@@ -253,16 +253,32 @@ __device__ __forceinline__ void insert_key(uint64_t top[8], uint64_t key) {
     }
 }
 
+// The column sums run two block columns at a time, c and c + 4, as the two
+// halves of one f32x2 register: each half subtracts the same source value
+// (duplicated into both halves) from its own block column and accumulates
+// its own even-row and odd-row chain, so every sum carries exactly the
+// scalar bits; cur_p holds the block's values interleaved that way,
+// cur_p[2 * (8 * cp + i) + h] = block column cp + 4h, row i. The tree runs on
+// the same pairs: {P01, P45} = {S0, S4}(j-1) + {S1, S5}(j), {P23, P67} =
+// {S2, S6}(j-1) + {S3, S7}(j), {Q0123, Q4567} = {P01, P45} + {P23, P67}.
+__device__ __forceinline__ unsigned long long add_f32x2(unsigned long long a, unsigned long long b) {
+    unsigned long long r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
 template <int K>
-__device__ __forceinline__ void scan_chunk_exact(const Region& reg, const float* cur_s,
+__device__ __forceinline__ void scan_chunk_exact(const Region& reg, const float* cur_p,
                                                  const Window& win, int r0, int nrows, int jcount,
                                                  uint64_t top[8]) {
-    float s0p[K], s2p[K], s4p[K], s6p[K];  // S0, S2, S4, S6 of the previous step
-    float p01[K][2], p45[K][2], q0123[K][4];
+    using u64 = unsigned long long;
+    u64 s04p[K], s26p[K];  // {S0, S4} and {S2, S6} of the previous step
+    u64 p0145[K][2];       // {P01, P45}, made two steps ago and one step ago
+    float q0123[K][4];     // Q0123, made up to four steps ago
 #pragma unroll
     for (int q = 0; q < K; ++q) {
-        s0p[q] = s2p[q] = s4p[q] = s6p[q] = 0.0f;
-        p01[q][0] = p01[q][1] = p45[q][0] = p45[q][1] = 0.0f;
+        s04p[q] = s26p[q] = 0ull;
+        p0145[q][0] = p0145[q][1] = 0ull;
 #pragma unroll
         for (int i = 0; i < 4; ++i) q0123[q][i] = 0.0f;
     }
@@ -270,44 +286,52 @@ __device__ __forceinline__ void scan_chunk_exact(const Region& reg, const float*
     const float* sbase = reg.smem + (r0 - reg.ry0) - reg.rx0 * reg.cs;
     const int cs = reg.cs;
     const int seq0 = win.seq_base + (r0 - win.top) * win.rw;
+    const u64* bpair = reinterpret_cast<const u64*>(cur_p);
 
     for (int j0 = 0; j0 < jcount; j0 += 4) {
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
             const int j = j0 + u;
-            float w[K + 7];
+            u64 wd[K + 7];  // source values, each in both halves
             {
                 const float* col = sbase + min(win.left + j, xmax) * cs;
 #pragma unroll
-                for (int k = 0; k < K + 7; ++k) w[k] = col[k];
+                for (int k = 0; k < K + 7; ++k) wd[k] = pack_f32x2(col[k], col[k]);
             }
-            float S[K][8];
+            u64 S[K][4];  // {S_cp, S_cp+4}
 #pragma unroll
-            for (int c = 0; c < 8; ++c) {
-                float b[8];
+            for (int cp = 0; cp < 4; ++cp) {
+                u64 b[8];
 #pragma unroll
-                for (int i = 0; i < 8; ++i) b[i] = cur_s[c * 8 + i];
+                for (int i = 0; i < 8; ++i) b[i] = bpair[8 * cp + i];
 #pragma unroll
-                for (int q = 0; q < K; ++q) S[q][c] = column_ssd_at<K>(b, w, q);
+                for (int q = 0; q < K; ++q) {
+                    u64 ev = 0ull, od = 0ull;  // {+0.0f, +0.0f}
+#pragma unroll
+                    for (int i = 0; i < 8; i += 2) {
+                        u64 d;
+                        asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(b[i]), "l"(wd[q + i]));
+                        asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(ev) : "l"(d), "l"(ev));
+                        asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(b[i + 1]), "l"(wd[q + i + 1]));
+                        asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(od) : "l"(d), "l"(od));
+                    }
+                    S[q][cp] = add_f32x2(ev, od);
+                }
             }
             float e[K];
 #pragma unroll
             for (int q = 0; q < K; ++q) {
-                const float np01 = __fadd_rn(s0p[q], S[q][1]);
-                const float np23 = __fadd_rn(s2p[q], S[q][3]);
-                const float np45 = __fadd_rn(s4p[q], S[q][5]);
-                const float np67 = __fadd_rn(s6p[q], S[q][7]);
+                const u64 np0145 = add_f32x2(s04p[q], S[q][1]);  // {P01, P45}(j-1), (j-5)
+                const u64 np2367 = add_f32x2(s26p[q], S[q][3]);  // {P23, P67}(j-3), (j-7)
                 // P01(j-3) and P45(j-7) were made two steps ago, Q0123(j-7) four
-                const float nq0123 = __fadd_rn(p01[q][u & 1], np23);
-                const float nq4567 = __fadd_rn(p45[q][u & 1], np67);
+                const u64 nq = add_f32x2(p0145[q][u & 1], np2367);  // {Q0123(j-3), Q4567(j-7)}
+                float nq0123, nq4567;
+                asm("mov.b64 {%0, %1}, %2;" : "=f"(nq0123), "=f"(nq4567) : "l"(nq));
                 e[q] = __fadd_rn(q0123[q][u & 3], nq4567);
-                p01[q][u & 1] = np01;
-                p45[q][u & 1] = np45;
+                p0145[q][u & 1] = np0145;
                 q0123[q][u & 3] = nq0123;
-                s0p[q] = S[q][0];
-                s2p[q] = S[q][2];
-                s4p[q] = S[q][4];
-                s6p[q] = S[q][6];
+                s04p[q] = S[q][0];
+                s26p[q] = S[q][2];
             }
             const int d = j - 7;
             if (d >= 0 && d < win.rw && j < jcount) {
@@ -604,8 +628,9 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
         const int jcount = warp_max(has ? win.rw + 7 : 8);
         if (kExact) {
             switch (K) {
-                case 2: scan_chunk_exact<2>(reg, cur_s, win, r0, nrows, jcount, top); break;
-                default: scan_chunk_exact<3>(reg, cur_s, win, r0, nrows, jcount, top); break;
+                // E: the block interleaved by column pairs (see scan_chunk_exact)
+                case 2: scan_chunk_exact<2>(reg, E, win, r0, nrows, jcount, top); break;
+                default: scan_chunk_exact<3>(reg, E, win, r0, nrows, jcount, top); break;
             }
         } else {
             switch (K) {
@@ -682,8 +707,9 @@ __host__ __device__ inline SmemPlan smem_plan(const StackJob& job, int mode) {
     const int h = tile_h + 2 * reach < job.height ? tile_h + 2 * reach : job.height;
     const int cs = (h + kMaxK + 7) | 1;
     p.region_floats = cs * w;
-    // the exact scan (radius >= 3) selects without error tables
-    p.estride = job.radius >= 3 ? 0 : ((error_table_floats(job) + 31) & ~31) + 8;
+    // the exact scan (radius >= 3) selects without error tables; its table
+    // area holds the block interleaved by column pairs (64 floats)
+    p.estride = job.radius >= 3 ? 64 : ((error_table_floats(job) + 31) & ~31) + 8;
     p.etab_floats = kGroups * p.estride;
     if (mode != kTableOnly && p.etab_floats < kGroups * kGroupStride)
         p.etab_floats = kGroups * kGroupStride;
@@ -743,6 +769,12 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
     float c7[8];
 #pragma unroll
     for (int i = 0; i < 8; ++i) c7[i] = cur_s[56 + i];
+    if (kExact) {
+        // block column c at pair c & 3, half c >> 2 (scan_chunk_exact)
+#pragma unroll
+        for (int i = 0; i < 8; ++i) E[2 * (8 * (sub & 3) + i) + (sub >> 2)] = cur_s[sub * 8 + i];
+        __syncwarp(gmask);
+    }
 
     auto stage = [&](const float* frame, int reach) {
         Region s;
