@@ -100,6 +100,9 @@ struct BatchWork {
 // status and enqueues on `stream`.
 cudaError_t launch_match(const StackJob& job, cudaStream_t stream);
 cudaError_t launch_filter(const StackJob& job, cudaStream_t stream);
+// The filter in CTAs of 8 groups, small enough to share an SM with a
+// matcher CTA: the engine runs it beside the next stack's matching.
+cudaError_t launch_filter_beside_match(const StackJob& job, cudaStream_t stream);
 const char* tile_shape_name(TileShape shape);
 bool tile_shape_fits(const StackJob& job, TileShape shape, TileMode mode);
 int default_tile_shape(const StackJob& job, TileMode mode);  // -1: none fits

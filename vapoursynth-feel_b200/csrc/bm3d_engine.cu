@@ -488,11 +488,12 @@ struct vsfeel_bm3d {
     // bits into its record instead of the context's match buffers.
     // frame_ptr: the search clip (the ref clip in the final pass); input_ptr:
     // the clip denoised in the final pass (its frames share frame_ptr's pitch)
-    void launch_stack(int m, const std::function<const float*(int)>& frame_ptr, int in_pitch,
-                      int out_lo, int out_hi, cudaStream_t st, unsigned char* saved = nullptr,
-                      bool table_only = false,
-                      const std::function<const float*(int)>* input_ptr = nullptr,
-                      float* own_slices = nullptr) {
+    // The StackJob of stack m; its match table goes to (table_xy, table_z)
+    // unless `saved` gives the stack's record.
+    StackJob stack_job(int m, const std::function<const float*(int)>& frame_ptr, int in_pitch,
+                       int out_lo, int out_hi, unsigned char* saved,
+                       const std::function<const float*(int)>* input_ptr, float* own_slices,
+                       uint32_t* table_xy, uint32_t* table_z) {
         const int r = s.radius;
         StackJob job{};
         for (int z = 0; z < tw(); ++z) {
@@ -521,8 +522,8 @@ struct vsfeel_bm3d {
         job.thr = s.thr;
         job.wiener = (s.final_pass && input_ptr) ? 1 : 0;
         job.extractor = s.extractor;
-        job.match_xy = match_xy.p;
-        job.match_z = match_z.p;
+        job.match_xy = table_xy;
+        job.match_z = table_z;
         job.mask_out = nullptr;
         if (saved) {
             const SavedLayout L = saved_layout();
@@ -532,6 +533,16 @@ struct vsfeel_bm3d {
             job.mask_out = reinterpret_cast<uint64_t*>(rec + L.off_mask);
         }
         job.status = status_word();
+        return job;
+    }
+
+    void launch_stack(int m, const std::function<const float*(int)>& frame_ptr, int in_pitch,
+                      int out_lo, int out_hi, cudaStream_t st, unsigned char* saved = nullptr,
+                      bool table_only = false,
+                      const std::function<const float*(int)>* input_ptr = nullptr,
+                      float* own_slices = nullptr) {
+        const StackJob job = stack_job(m, frame_ptr, in_pitch, out_lo, out_hi, saved, input_ptr,
+                                       own_slices, match_xy.p, match_z.p);
         // fused: one tiled launch matches and filters (the match table stays
         // on chip); otherwise the match table goes through global memory
         if (table_only) {
@@ -582,15 +593,47 @@ struct vsfeel_bm3d {
         launches += 1;
     }
 
+    // Second stream of the overlapped schedule (see run) and its events:
+    // ev_match[b] after the matching that wrote table buffer b, ev_filter[b]
+    // after the filtering that read it.
+    cudaStream_t filter_stream = nullptr, match_stream = nullptr;
+    cudaEvent_t ev_match[2] = {}, ev_filter[2] = {}, ev_fork = nullptr, ev_join = nullptr,
+                ev_join_match = nullptr;
+    DevBuf<uint32_t> match_xy2, match_z2;
+    bool overlap = true;  // VSFEEL_OVERLAP_FILTER=0: one stream, as the fused mode
+    void overlap_setup() {
+        if (filter_stream) return;
+        int least = 0, greatest = 0;
+        VSF_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        VSF_CUDA(cudaStreamCreateWithPriority(&match_stream, cudaStreamNonBlocking, greatest));
+        VSF_CUDA(cudaStreamCreateWithPriority(&filter_stream, cudaStreamNonBlocking, least));
+        for (cudaEvent_t* e : {&ev_match[0], &ev_match[1], &ev_filter[0], &ev_filter[1], &ev_fork,
+                               &ev_join, &ev_join_match})
+            VSF_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+    }
+
     // Denoises outputs [first, first+count) from device frames.
-    // before_stack(m) runs before stack m is launched, after_output(n) after
-    // output n's normalisation is enqueued (the host path's copy overlap).
+    // before_stack(m, s) runs before stack m is launched on stream s,
+    // after_output(n, s) after output n's normalisation is enqueued on stream
+    // s (the host path's copy overlap). All work is ordered after the prior
+    // work of st, and st waits for all of it at the end.
+    //
+    // Overlapped schedule (the default with separate match and filter
+    // kernels): stack m's filtering, the clearing of its outputs' slots and
+    // their normalisation run on a second stream, beside stack m+1's
+    // matching. The matcher leaves room on each SM for one filter CTA of 8
+    // groups (launch_filter_beside_match), so the filter's gathers and
+    // atomics overlap the matcher's issue-bound work. The matching runs on a
+    // stream of the highest priority and the filtering on one of the lowest,
+    // so that an SM a matcher CTA leaves goes to the next matcher CTA, not to
+    // more filter CTAs. Match tables alternate between two buffers: stack
+    // m+2's matching waits for stack m's filter.
     void run(const std::function<const float*(int)>& frame_ptr, int in_pitch,
              const std::function<float*(int)>& out_ptr, int out_pitch, int first, int count,
              cudaStream_t st, unsigned char* saved = nullptr,
              const std::function<const float*(int)>* input_ptr = nullptr,
-             const std::function<void(int)>* before_stack = nullptr,
-             const std::function<void(int)>* after_output = nullptr) {
+             const std::function<void(int, cudaStream_t)>* before_stack = nullptr,
+             const std::function<void(int, cudaStream_t)>* after_output = nullptr) {
         if (count <= 0) return;
         const int r = s.radius;
         const int last = first + count - 1;
@@ -600,20 +643,59 @@ struct vsfeel_bm3d {
         const int m_lo = clampf(first - r), m_hi = clampf(last + r);
         int zeroed = first - 1;     // highest output whose slot is zeroed
         int finished = first - 1;   // highest output normalised
+        const bool two = overlap && !fused;
+        cudaStream_t fs = st;  // filter, slot clearing, normalisation
+        cudaStream_t ms = st;  // matching
+        if (two) {
+            overlap_setup();
+            match_xy2.ensure((size_t)nblocks * 8);
+            match_z2.ensure((size_t)nblocks);
+            fs = filter_stream;
+            ms = match_stream;
+            VSF_CUDA(cudaEventRecord(ev_fork, st));
+            VSF_CUDA(cudaStreamWaitEvent(fs, ev_fork, 0));
+            VSF_CUDA(cudaStreamWaitEvent(ms, ev_fork, 0));
+        }
         for (int m = m_lo; m <= m_hi; ++m) {
             const int want = std::min(last, m + r);
-            for (int n = zeroed + 1; n <= want; ++n)
-                VSF_CUDA(cudaMemsetAsync(slot_pair(n, 0), 0,
-                                         sizeof(float) * (size_t)tw() * 2 * acc_plane, st));
-            zeroed = std::max(zeroed, want);
-            if (before_stack) (*before_stack)(m);
-            launch_stack(m, frame_ptr, in_pitch, first, last, st, saved, false, input_ptr);
+            if (!two) {
+                for (int n = zeroed + 1; n <= want; ++n)
+                    VSF_CUDA(cudaMemsetAsync(slot_pair(n, 0), 0,
+                                             sizeof(float) * (size_t)tw() * 2 * acc_plane, st));
+                zeroed = std::max(zeroed, want);
+                if (before_stack) (*before_stack)(m, st);
+                launch_stack(m, frame_ptr, in_pitch, first, last, st, saved, false, input_ptr);
+            } else {
+                const int b = (m - m_lo) & 1;
+                // stack m-2's filter has read this table buffer
+                if (m - m_lo >= 2) VSF_CUDA(cudaStreamWaitEvent(ms, ev_filter[b], 0));
+                if (before_stack) (*before_stack)(m, ms);
+                const StackJob job =
+                    stack_job(m, frame_ptr, in_pitch, first, last, saved, input_ptr, nullptr,
+                              b ? match_xy2.p : match_xy.p, b ? match_z2.p : match_z.p);
+                traced(VSFEEL_KERNEL_MATCH, ms, [&] { return launch_match(job, ms); });
+                VSF_CUDA(cudaEventRecord(ev_match[b], ms));
+                VSF_CUDA(cudaStreamWaitEvent(fs, ev_match[b], 0));
+                for (int n = zeroed + 1; n <= want; ++n)
+                    VSF_CUDA(cudaMemsetAsync(slot_pair(n, 0), 0,
+                                             sizeof(float) * (size_t)tw() * 2 * acc_plane, fs));
+                zeroed = std::max(zeroed, want);
+                traced(VSFEEL_KERNEL_FILTER, fs, [&] { return launch_filter_beside_match(job, fs); });
+                VSF_CUDA(cudaEventRecord(ev_filter[b], fs));
+                launches += 2;
+            }
             const int done = (m == m_hi) ? last : std::min(last, m - r);
             for (int n = finished + 1; n <= done; ++n) {
-                launch_normalize(n, out_ptr(n), out_pitch, st, saved);
-                if (after_output) (*after_output)(n);
+                launch_normalize(n, out_ptr(n), out_pitch, fs, saved);
+                if (after_output) (*after_output)(n, fs);
             }
             finished = std::max(finished, done);
+        }
+        if (two) {
+            VSF_CUDA(cudaEventRecord(ev_join, fs));
+            VSF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
+            VSF_CUDA(cudaEventRecord(ev_join_match, ms));
+            VSF_CUDA(cudaStreamWaitEvent(st, ev_join_match, 0));
         }
     }
 
@@ -726,6 +808,7 @@ int vsfeel_bm3d_create_plane(const vsfeel_bm3d_args* args, const vsfeel_bm3d_vid
     ctx->acc_pitch = (s.width + 31) & ~31;
     ctx->acc_plane = (size_t)s.height * ctx->acc_pitch;
     if (const char* v = std::getenv("VSFEEL_FUSED_FILTER")) ctx->fused = v[0] == '1';
+    if (const char* v = std::getenv("VSFEEL_OVERLAP_FILTER")) ctx->overlap = v[0] != '0';
     DeviceGuard dg(device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
@@ -744,12 +827,17 @@ void vsfeel_bm3d_free(vsfeel_bm3d* ctx) {
             wait_stream(ctx->stream, timeout_ms());
             cudaStreamDestroy(ctx->stream);
         }
-        for (cudaStream_t cs : {ctx->up_stream, ctx->down_stream})
+        for (cudaStream_t cs : {ctx->up_stream, ctx->down_stream, ctx->filter_stream, ctx->match_stream})
             if (cs) {
                 wait_stream(cs, timeout_ms());
                 cudaStreamDestroy(cs);
             }
         if (ctx->tail) cudaEventDestroy(ctx->tail);
+        for (cudaEvent_t e : {ctx->ev_match[0], ctx->ev_match[1], ctx->ev_filter[0], ctx->ev_filter[1],
+                              ctx->ev_fork, ctx->ev_join, ctx->ev_join_match})
+            if (e) cudaEventDestroy(e);
+        ctx->match_xy2.release();
+        ctx->match_z2.release();
         for (cudaEvent_t e : ctx->frame_events) cudaEventDestroy(e);
         for (cudaEvent_t e : ctx->out_events) cudaEventDestroy(e);
         ctx->ring.release();
@@ -958,10 +1046,10 @@ int process_host(vsfeel_bm3d* ctx, const float* src, ptrdiff_t src_frame_stride_
             }
             uploaded = std::max(uploaded, f_need);
         };
-        const std::function<void(int)> before = [&](int m) {
+        const std::function<void(int, cudaStream_t)> before = [&](int m, cudaStream_t ms) {
             const int f_need = std::min(ctx->clampf(m + r), f_hi);
             upload_to(f_need);
-            VSF_CUDA(cudaStreamWaitEvent(st, ctx->frame_events[f_need - f_lo], 0));
+            VSF_CUDA(cudaStreamWaitEvent(ms, ctx->frame_events[f_need - f_lo], 0));
         };
         // Downloads: into page-locked memory each output goes down as soon as
         // it is normalised; into pageable memory (whose copies would block the
@@ -977,14 +1065,14 @@ int process_host(vsfeel_bm3d* ctx, const float* src, ptrdiff_t src_frame_stride_
                                        sizeof(float) * ctx->acc_pitch, row_bytes, s.height,
                                        cudaMemcpyDeviceToHost, cs));
         };
-        const std::function<void(int)> after = [&](int n) {
-            VSF_CUDA(cudaEventRecord(ctx->out_events[n - first], st));
+        const std::function<void(int, cudaStream_t)> after = [&](int n, cudaStream_t ns) {
+            VSF_CUDA(cudaEventRecord(ctx->out_events[n - first], ns));
             VSF_CUDA(cudaStreamWaitEvent(ctx->down_stream, ctx->out_events[n - first], 0));
             download(n, ctx->down_stream);
         };
         auto src_at = [&](int f) -> const float* { return src_base + (size_t)(f - f_lo) * ff; };
         auto out_at = [&](int n) { return ctx->outbuf.p + (size_t)(n - first) * ff; };
-        const std::function<void(int)>* after_ptr = pinned_dst ? &after : nullptr;
+        const std::function<void(int, cudaStream_t)>* after_ptr = pinned_dst ? &after : nullptr;
         if (!ref) {
             ctx->run(src_at, ctx->acc_pitch, out_at, ctx->acc_pitch, first, count, st, nullptr,
                      nullptr, &before, after_ptr);

@@ -261,11 +261,13 @@ __global__ void __launch_bounds__(128) bm3d_match_kernel(const StackJob job) {
     }
 }
 
-// The standalone filter: 16 groups of 8 lanes per CTA, matches read from
-// the stack's match table.
-template <bool kSaveMask, bool kWiener>
-__global__ void __launch_bounds__(128) bm3d_filter_kernel(const StackJob job) {
-    __shared__ float smem[kFilterGroupsPerCta * kGroupStride];
+// The standalone filter: kGroups groups of 8 lanes per CTA, matches read
+// from the stack's match table. 16 groups when it runs alone; 8 when it
+// runs beside the next stack's matching, so that one CTA fits on an SM next
+// to a matcher CTA (18.7 KB of shared memory, 64 threads).
+template <bool kSaveMask, bool kWiener, int kGroups = kFilterGroupsPerCta>
+__global__ void __launch_bounds__(kGroups * 8) bm3d_filter_kernel(const StackJob job) {
+    __shared__ float smem[kGroups * kGroupStride];
     const int sub = threadIdx.x & 7;
     float* buf = smem + (threadIdx.x >> 3) * kGroupStride;
     const int nblocks = job.nbx * job.nby;
@@ -479,6 +481,18 @@ cudaError_t launch_filter(const StackJob& job, cudaStream_t stream) {
         bm3d_filter_kernel<true, false><<<block_grid(job), kThreads, 0, stream>>>(job);
     else
         bm3d_filter_kernel<false, false><<<block_grid(job), kThreads, 0, stream>>>(job);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_filter_beside_match(const StackJob& job, cudaStream_t stream) {
+    constexpr int kSmall = 8, kSmallThreads = kSmall * 8;
+    const int grid = (job.nbx * job.nby * 8 + kSmallThreads - 1) / kSmallThreads;
+    if (job.wiener)
+        bm3d_filter_kernel<false, true, kSmall><<<grid, kSmallThreads, 0, stream>>>(job);
+    else if (job.mask_out)
+        bm3d_filter_kernel<true, false, kSmall><<<grid, kSmallThreads, 0, stream>>>(job);
+    else
+        bm3d_filter_kernel<false, false, kSmall><<<grid, kSmallThreads, 0, stream>>>(job);
     return cudaGetLastError();
 }
 

@@ -699,6 +699,11 @@ __device__ void stage_region(float* smem, const float* __restrict__ frame, int p
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// windows a block holds at once: the spatial one, or ps_num temporal ones
+__host__ __device__ inline int window_slots(const StackJob& job) {
+    return job.ps_num > 1 ? job.ps_num : 1;
+}
+
 struct SmemPlan {
     int region_floats;  // staged region
     int estride;        // floats per block error table (== 8 mod 32)
@@ -721,16 +726,18 @@ __host__ __device__ inline SmemPlan smem_plan(const StackJob& job, int mode) {
     const int tile_w = (TX - 1) * job.step + 8, tile_h = (TY - 1) * job.step + 8;
     const int w = tile_w + 2 * reach < job.width ? tile_w + 2 * reach : job.width;
     const int h = tile_h + 2 * reach < job.height ? tile_h + 2 * reach : job.height;
-    const int cs = (h + kMaxK + 7) | 1;
+    // rows past the region that masked chunk rows read: at most kMaxK - 1
+    const int cs = (h + kMaxK - 1) | 1;
     p.region_floats = cs * w;
     // the exact scan (radius >= 3) selects without error tables; its table
     // area holds the block interleaved by column pairs (64 floats)
-    p.estride = job.radius >= 3 ? 64 : ((error_table_floats(job) + 31) & ~31) + 8;
+    const int tf = error_table_floats(job);
+    p.estride = job.radius >= 3 ? 64 : tf + ((8 - tf) & 31);  // the least >= tf that is 8 mod 32
     p.etab_floats = kGroups * p.estride;
     if (mode != kTableOnly && p.etab_floats < kGroups * kGroupStride)
         p.etab_floats = kGroups * kGroupStride;
     p.bytes = sizeof(float) * (size_t(kGroups) * 64 + size_t(p.etab_floats) + p.region_floats) +
-              sizeof(Window) * kGroups * 8 + sizeof(GroupState) * kGroups;
+              sizeof(Window) * kGroups * window_slots(job) + sizeof(GroupState) * kGroups;
     return p;
 }
 
@@ -745,7 +752,7 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
     const SmemPlan plan = smem_plan<TX, TY>(job, kMode);
     GroupState* gs_all = reinterpret_cast<GroupState*>(smem_raw);
     Window* win_all = reinterpret_cast<Window*>(gs_all + kGroups);
-    float* cur_all = reinterpret_cast<float*>(win_all + kGroups * 8);
+    float* cur_all = reinterpret_cast<float*>(win_all + kGroups * window_slots(job));
     float* etab_all = cur_all + kGroups * 64;
     float* region = etab_all + (size_t)plan.etab_floats;
 
@@ -776,7 +783,7 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
 
     float* cur_s = cur_all + g * 64;
     float* E = etab_all + (size_t)g * plan.estride;
-    Window* win = win_all + g * 8;
+    Window* win = win_all + g * window_slots(job);
     GroupState* gs = gs_all + g;
     const float* fc = job.slice_frame[r];
 #pragma unroll
@@ -799,7 +806,9 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         const int ry0 = max(tile_y0 - reach, 0);
         const int ry1 = min(tile_y1 + reach, H - 8) + 7;
         // column: the region's rows plus the rows masked chunk rows may read
-        s.cs = (ry1 - ry0 + 1 + kMaxK + 7) | 1;
+        // (a chunk starts at or above the window's last row and reads K + 6
+        // rows below its start: at most kMaxK - 1 past the region)
+        s.cs = (ry1 - ry0 + 1 + kMaxK - 1) | 1;
         s.rx0 = rx0;
         s.ry0 = ry0;
         s.rx1 = rx1;
