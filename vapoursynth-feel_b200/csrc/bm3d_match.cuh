@@ -93,13 +93,23 @@ __device__ __forceinline__ Window make_window(int cx, int cy, int range, int wid
     return w;
 }
 
-// The staged region, column-major with column stride cs (odd), so the K+7
-// source rows a lane needs at one column are consecutive words.
+// The staged region. The exact scan stages it column-major with column
+// stride cs (odd), so the K+7 source rows a lane needs at one column are
+// consecutive words. The sliding scan stages it row-major with row stride
+// rs (even, 2 mod 4, one column of padding), so the columns X and X+1 of a
+// row (X even) form one 8-byte pair.
 struct Region {
     const float* smem;
     int rx0, ry0, cs;
     int rx1, ry1;  // last staged column and row
+    int rs;
 };
+
+__host__ __device__ inline int row_stride(int w) {
+    int rs = (w + 2) & ~1;
+    if ((rs & 3) == 0) rs += 2;
+    return rs;
+}
 
 __device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi) {
     unsigned long long r;
@@ -107,112 +117,106 @@ __device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi) {
     return r;
 }
 
-// SSD of one column of the block (bc) against w[q..q+7]: the even-row and
-// odd-row sums advance together as one packed pair ({even, odd}) with the
-// sm_100 f32x2 subtract and fused multiply-add, each half rounded exactly as
-// the scalar e += d*d of the reference's two chains.
-template <int K>
-__device__ __forceinline__ float column_ssd_at(const float bc[8], const float w[K + 7], int q) {
-    unsigned long long acc = 0ull;  // {+0.0f, +0.0f}
-#pragma unroll
-    for (int i = 0; i < 8; i += 2) {
-        unsigned long long d;
-        asm("sub.rn.f32x2 %0, %1, %2;"
-            : "=l"(d)
-            : "l"(pack_f32x2(bc[i], bc[i + 1])), "l"(pack_f32x2(w[q + i], w[q + i + 1])));
-        asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(acc) : "l"(d), "l"(acc));
-    }
-    float ev, od;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(ev), "=f"(od) : "l"(acc));
-    return __fadd_rn(ev, od);
-}
-
 // One lane's chunk: rows r0..r0+nrows-1 of window `win` (nrows may be 0),
 // `jcount` column steps (warp-uniform; steps past the window's width are
 // padding). cur_s: the block's 64 values in shared memory, column-major; c7:
 // block column 7 in registers. Errors go to table E; each row's two smallest
 // errors are merged into lb, this lane's 8 smallest such values (ascending).
+//
+// The sweep takes two steps at a time: source columns X and X+1 (X even in
+// the row-major region; a window starting at an odd column starts one
+// column early, on a step whose sums no candidate uses) are one 8-byte pair
+// per row, and V(j), V(j+1) are the two halves of one f32x2 register, each
+// half running the scalar even-row and odd-row chains against block columns
+// min(j, 7) and min(j+1, 7). Per row the tree then advances two candidates
+// on the reference's operands: P(j-1) = V(j-1) + V(j), P(j) = V(j) + V(j+1),
+// Q(j-3) = P(j-3) + P(j-1), Q(j-2) = P(j-2) + P(j), E(j-7) = Q(j-7) + Q(j-3),
+// E(j-6) = Q(j-6) + Q(j-2).
 template <int K>
 __device__ __forceinline__ void scan_chunk(const Region& reg, const float* cur_s, const float c7[8],
                                            const Window& win, int r0, int nrows, int jcount,
                                            float* E, float lb[8]) {
-    float vp[K], pr[K][2], qr[K][4];
+    using u64 = unsigned long long;
     float m1[K], m2[K];
+    float vprev[K], pa[K], pb[K], qa[K][2], qb[K][2];
 #pragma unroll
-    for (int q = 0; q < K; ++q) m1[q] = m2[q] = kFltMax;
-    const int xmax = win.left + win.rw + 6;
-    // rows past the window exist in each staged column (padding) and only
-    // feed masked rows
-    const float* sbase = reg.smem + (r0 - reg.ry0) - reg.rx0 * reg.cs;
-    const int cs = reg.cs;
+    for (int q = 0; q < K; ++q) {
+        m1[q] = m2[q] = kFltMax;
+        vprev[q] = pa[q] = pb[q] = 0.0f;
+        qa[q][0] = qa[q][1] = qb[q][0] = qb[q][1] = 0.0f;
+    }
+    const int xs = win.left - reg.rx0;    // the window's first source column
+    const int jst = -(xs & 1);            // first step: an even column
+    const int xlast = (xs + win.rw + 6) & ~1;  // last pair holding a needed column
+    // rows past the window exist in the region (padding) and only feed masked rows
+    const float* rbase = reg.smem + (r0 - reg.ry0) * reg.rs;
+    const int rs = reg.rs;
     float* ecol = E + win.eoff + (r0 - win.top);
+    const int npairs = (jcount + 2) >> 1;
 
-    auto load_col = [&](int X, float w[K + 7]) {
-        const float* col = sbase + X * cs;
-#pragma unroll
-        for (int k = 0; k < K + 7; ++k) w[k] = col[k];
-    };
-    auto emit = [&](const float e[K], int d) {
-        if (d < win.rw) {
-            float* out = ecol + d * win.h;
-#pragma unroll
-            for (int q = 0; q < K; ++q) {
-                if (q < nrows) {
-                    out[q] = e[q];
-                    m2[q] = fminf(m2[q], fmaxf(m1[q], e[q]));
-                    m1[q] = fminf(m1[q], e[q]);
-                }
-            }
+    auto emit = [&](float e, int q, int d) {
+        if (q < nrows && d >= 0 && d < win.rw) {
+            ecol[d * win.h + q] = e;
+            m2[q] = fminf(m2[q], fmaxf(m1[q], e));
+            m1[q] = fminf(m1[q], e);
         }
     };
-
-    // warm-up: block columns 0..7, steps j = 0..7 (candidate column 0 at j = 7)
+    // iteration t: steps j = jst + 2t and j + 1 against the block pairs b
+    auto step = [&](int t, const u64 b[8], int ring) {
+        const int j = jst + 2 * t;
+        const int X = min(xs + j, xlast);
+        u64 w[K + 7];
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        float bc[8];
-#pragma unroll
-        for (int i = 0; i < 8; ++i) bc[i] = (j == 7) ? c7[i] : cur_s[j * 8 + i];
-        float w[K + 7];
-        load_col(min(win.left + j, xmax), w);
-        float e[K];
+        for (int k = 0; k < K + 7; ++k) w[k] = *reinterpret_cast<const u64*>(rbase + k * rs + X);
 #pragma unroll
         for (int q = 0; q < K; ++q) {
-            const float v = column_ssd_at<K>(bc, w, q);
-            e[q] = 0.0f;
-            if (j >= 1) {
-                const float np = __fadd_rn(vp[q], v);  // P(j-1)
-                if (j >= 3) {
-                    const float nq = __fadd_rn(pr[q][(j + 1) & 1], np);  // Q(j-3)
-                    if (j == 7) e[q] = __fadd_rn(qr[q][0], nq);          // E(0)
-                    qr[q][(j + 1) & 3] = nq;
-                }
-                pr[q][(j + 1) & 1] = np;
+            u64 ev = 0ull, od = 0ull;  // {+0.0f, +0.0f}
+#pragma unroll
+            for (int i = 0; i < 8; i += 2) {
+                u64 d;
+                asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(b[i]), "l"(w[q + i]));
+                asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(ev) : "l"(d), "l"(ev));
+                asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(b[i + 1]), "l"(w[q + i + 1]));
+                asm("fma.rn.f32x2 %0, %1, %1, %2;" : "=l"(od) : "l"(d), "l"(od));
             }
-            vp[q] = v;
+            u64 v;
+            asm("add.rn.f32x2 %0, %1, %2;" : "=l"(v) : "l"(ev), "l"(od));
+            float va, vb;
+            asm("mov.b64 {%0, %1}, %2;" : "=f"(va), "=f"(vb) : "l"(v));
+            const float p_a = __fadd_rn(vprev[q], va);  // P(j-1)
+            const float p_b = __fadd_rn(va, vb);        // P(j)
+            const float q_a = __fadd_rn(pa[q], p_a);    // Q(j-3)
+            const float q_b = __fadd_rn(pb[q], p_b);    // Q(j-2)
+            const float e_a = __fadd_rn(qa[q][ring], q_a);  // E(j-7)
+            const float e_b = __fadd_rn(qb[q][ring], q_b);  // E(j-6)
+            vprev[q] = vb;
+            pa[q] = p_a;
+            pb[q] = p_b;
+            qa[q][ring] = q_a;
+            qb[q][ring] = q_b;
+            emit(e_a, q, j - 7);
+            emit(e_b, q, j - 6);
         }
-        if (j == 7) emit(e, 0);
+    };
+
+    // warm-up: iterations 0..3 cover steps up to 7 (block columns j, j+1,
+    // clamped to 0..7, per lane as its first step is 0 or -1)
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const int ca = max(jst + 2 * t, 0), cb = jst + 2 * t + 1;
+        u64 b[8];
+#pragma unroll
+        for (int i = 0; i < 8; ++i) b[i] = pack_f32x2(cur_s[ca * 8 + i], cur_s[cb * 8 + i]);
+        step(t, b, t & 1);
     }
-    // steady state: block column 7, steps j = 8 .. jcount-1, four per
-    // iteration so that the ring positions are static
-    for (int j0 = 8; j0 < jcount; j0 += 4) {
+    // steady state: block column 7 in both halves
+    u64 b7[8];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int j = j0 + u;
-            float w[K + 7];
-            load_col(min(win.left + j, xmax), w);
-            float e[K];
+    for (int i = 0; i < 8; ++i) b7[i] = pack_f32x2(c7[i], c7[i]);
+    for (int t0 = 4; t0 < npairs; t0 += 2) {
 #pragma unroll
-            for (int q = 0; q < K; ++q) {
-                const float v = column_ssd_at<K>(c7, w, q);
-                const float np = __fadd_rn(vp[q], v);
-                const float nq = __fadd_rn(pr[q][(u + 1) & 1], np);
-                e[q] = __fadd_rn(qr[q][(u + 1) & 3], nq);
-                pr[q][(u + 1) & 1] = np;
-                qr[q][(u + 1) & 3] = nq;
-                vp[q] = v;
-            }
-            if (j < jcount) emit(e, j - 7);
-        }
+        for (int u = 0; u < 2; ++u)
+            if (t0 + u < npairs) step(t0 + u, b7, u);
     }
     // merge the rows' two smallest into the lane's 8 smallest
 #pragma unroll
@@ -699,6 +703,23 @@ __device__ void stage_region(float* smem, const float* __restrict__ frame, int p
     asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
+// The same region row-major with row stride rs (the sliding scan).
+__device__ void stage_region_rows(float* smem, const float* __restrict__ frame, int pitch, int rx0,
+                                  int ry0, int rx1, int ry1, int rs) {
+    const int w = rx1 - rx0 + 1;
+    const int h = ry1 - ry0 + 1;
+    const int lane = threadIdx.x & 31;
+    for (int yy = threadIdx.x >> 5; yy < h; yy += blockDim.x >> 5) {
+        const float* __restrict__ row = frame + (size_t)(ry0 + yy) * pitch + rx0;
+        for (int xx = lane; xx < w; xx += 32) {
+            const unsigned dst = (unsigned)__cvta_generic_to_shared(smem + yy * rs + xx);
+            asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(row + xx)
+                         : "memory");
+        }
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
 // windows a block holds at once: the spatial one, or ps_num temporal ones
 __host__ __device__ inline int window_slots(const StackJob& job) {
     return job.ps_num > 1 ? job.ps_num : 1;
@@ -726,9 +747,10 @@ __host__ __device__ inline SmemPlan smem_plan(const StackJob& job, int mode) {
     const int tile_w = (TX - 1) * job.step + 8, tile_h = (TY - 1) * job.step + 8;
     const int w = tile_w + 2 * reach < job.width ? tile_w + 2 * reach : job.width;
     const int h = tile_h + 2 * reach < job.height ? tile_h + 2 * reach : job.height;
-    // rows past the region that masked chunk rows read: at most kMaxK - 1
+    // rows past the region that masked chunk rows read: at most kMaxK - 1;
+    // column-major for the exact scan, row-major for the sliding one
     const int cs = (h + kMaxK - 1) | 1;
-    p.region_floats = cs * w;
+    p.region_floats = job.radius >= 3 ? cs * w : row_stride(w) * (h + kMaxK - 1);
     // the exact scan (radius >= 3) selects without error tables; its table
     // area holds the block interleaved by column pairs (64 floats)
     const int tf = error_table_floats(job);
@@ -809,13 +831,17 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         // (a chunk starts at or above the window's last row and reads K + 6
         // rows below its start: at most kMaxK - 1 past the region)
         s.cs = (ry1 - ry0 + 1 + kMaxK - 1) | 1;
+        s.rs = row_stride(rx1 - rx0 + 1);
         s.rx0 = rx0;
         s.ry0 = ry0;
         s.rx1 = rx1;
         s.ry1 = ry1;
         s.smem = region;
         __syncthreads();  // the previous phase has finished with the region
-        stage_region(region, frame, pitch, rx0, ry0, rx1, ry1, s.cs);
+        if (kExact)
+            stage_region(region, frame, pitch, rx0, ry0, rx1, ry1, s.cs);
+        else
+            stage_region_rows(region, frame, pitch, rx0, ry0, rx1, ry1, s.rs);
         __syncthreads();
         return s;
     };
