@@ -92,6 +92,25 @@ def test_random_configs_vs_oracle(seed, oracle_lib):
     assert np.array_equal(_cuda_tables(frames, p, [m])[m], oracle_lib.matches(frames, p, m))
 
 
+@pytest.mark.parametrize("seed", range(100, 132))
+def test_many_small_random_configs_vs_oracle(seed, oracle_lib):
+    """Small frames and narrow windows: windows starting at odd and even
+    columns, windows narrower than 8, clamped at every edge, every
+    block_step and radius; match tables bit-exact, outputs within the bar."""
+    rng = np.random.default_rng(seed)
+    p = Params(sigma=float(rng.uniform(1.0, 10.0)), block_step=int(rng.integers(1, 9)),
+               bm_range=int(rng.integers(1, 12)), radius=int(rng.integers(0, 5)),
+               ps_num=int(rng.integers(1, 9)), ps_range=int(rng.integers(1, 6)),
+               extractor_exp=int(rng.choice([0, 0, 2])))
+    n = int(rng.integers(1, 2 * p.radius + 3))
+    h, w = int(rng.integers(8, 40)), int(rng.integers(8, 48))
+    frames = make_clip(n, h, w, sigma=p.sigma, shift=3, seed=5000 + seed)
+    out = _node(frames, **p.as_dict()).output()
+    assert np.abs(out.astype(np.float64) - oracle_lib.bm3d(frames, p)).max() <= OUT_TOL, p.as_dict()
+    for m in sorted({0, n - 1}):
+        assert np.array_equal(_cuda_tables(frames, p, [m])[m], oracle_lib.matches(frames, p, m)), m
+
+
 @pytest.mark.parametrize("kw", [
     dict(sigma=6.0, block_step=4, bm_range=20, radius=2, ps_num=2, ps_range=7),   # wide window
     dict(sigma=6.0, block_step=3, bm_range=8, radius=2, ps_num=8, ps_range=9),    # many windows
