@@ -550,7 +550,12 @@ def main() -> int:
                 "frac": achieved / peak, "traffic": traffic,
                 "kernel": "bm3d_match_kernel", "peak_source": peak_src,
                 "avg_launch_ms": avg_s * 1e3, "algorithmic_bytes_per_launch": alg_bytes,
-                "kernel_ms_share": {k: round(ms / max(sum(x[0] for x in kt.values()), 1e-9), 4)
+                # summed event spans per kernel kind; filtering and normalisation run
+                # on a second stream beside the matching, so their spans overlap it
+                # and include waiting for SM space (the ncu launch list in profiles/
+                # gives the serialised time shares)
+                "kernel_span_ms_per_step": {k: round(ms / args.steps, 3) for k, (ms, _) in kt.items()},
+                "kernel_span_share": {k: round(ms / max(sum(x[0] for x in kt.values()), 1e-9), 4)
                                     for k, (ms, _) in kt.items()}}
 
     if rank != 0:
