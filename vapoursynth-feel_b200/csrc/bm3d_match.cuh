@@ -17,12 +17,12 @@
 // the same additions on the same operands as
 // ((c0+c1)+(c2+c3))+((c4+c5)+(c6+c7)), so every candidate error carries the
 // reference's bits. Every error is stored to the block's error table in
-// shared memory; the lane also keeps each row's two smallest errors.
+// shared memory; the lane also keeps each row's three smallest errors.
 //
 // Selection. The reference keeps per-lane sorted top-8 lists and merges them
 // by (error, scan index); the result is the 8 smallest (error, index) keys.
 // Here the block's 8 lanes bound the 8th smallest error by the 8th smallest
-// of the window rows' two smallest errors, collect the few candidates at or
+// of the window rows' three smallest errors, collect the few candidates at or
 // below the bound from the table, and place each by counting the collected
 // keys below it. The scan itself carries no branches or votes.
 //
@@ -120,7 +120,7 @@ __device__ __forceinline__ unsigned long long pack_f32x2(float lo, float hi) {
 // One lane's chunk: rows r0..r0+nrows-1 of window `win` (nrows may be 0),
 // `jcount` column steps (warp-uniform; steps past the window's width are
 // padding). cur_s: the block's 64 values in shared memory, column-major; c7:
-// block column 7 in registers. Errors go to table E; each row's two smallest
+// block column 7 in registers. Errors go to table E; each row's three smallest
 // errors are merged into lb, this lane's 8 smallest such values (ascending).
 //
 // The sweep takes two steps at a time: source columns X and X+1 (X even in
@@ -137,11 +137,11 @@ __device__ __forceinline__ void scan_chunk(const Region& reg, const float* cur_s
                                            const Window& win, int r0, int nrows, int jcount,
                                            float* E, float lb[8]) {
     using u64 = unsigned long long;
-    float m1[K], m2[K];
+    float m1[K], m2[K], m3[K];
     float vprev[K], pa[K], pb[K], qa[K][2], qb[K][2];
 #pragma unroll
     for (int q = 0; q < K; ++q) {
-        m1[q] = m2[q] = kFltMax;
+        m1[q] = m2[q] = m3[q] = kFltMax;
         vprev[q] = pa[q] = pb[q] = 0.0f;
         qa[q][0] = qa[q][1] = qb[q][0] = qb[q][1] = 0.0f;
     }
@@ -157,6 +157,7 @@ __device__ __forceinline__ void scan_chunk(const Region& reg, const float* cur_s
     auto emit = [&](float e, int q, int d) {
         if (q < nrows && d >= 0 && d < win.rw) {
             ecol[d * win.h + q] = e;
+            m3[q] = fminf(m3[q], fmaxf(m2[q], e));
             m2[q] = fminf(m2[q], fmaxf(m1[q], e));
             m1[q] = fminf(m1[q], e);
         }
@@ -218,10 +219,12 @@ __device__ __forceinline__ void scan_chunk(const Region& reg, const float* cur_s
         for (int u = 0; u < 2; ++u)
             if (t0 + u < npairs) step(t0 + u, b7, u);
     }
-    // merge the rows' two smallest into the lane's 8 smallest
+    // merge the rows' three smallest into the lane's 8 smallest (three per
+    // row bound the 8th smallest tighter than two, so fewer candidates pass
+    // the selection's bound; a fourth costs more than it saves)
 #pragma unroll
-    for (int q = 0; q < 2 * K; ++q) {
-        float c = q < K ? m1[q] : m2[q - K];
+    for (int q = 0; q < 3 * K; ++q) {
+        float c = q < K ? m1[q] : (q < 2 * K ? m2[q - K] : m3[q - 2 * K]);
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
             const float lo = fminf(lb[i], c);
@@ -399,7 +402,7 @@ __device__ __forceinline__ void merge_top8(uint64_t top[8], GroupState* gs, unsi
 __device__ void select_top8(const float* E, const Window* wins, int nwin, float lb[8],
                             GroupState* gs, unsigned gmask) {
     const int sub = threadIdx.x & 7;
-    // bound: the 8th smallest of the rows' two smallest errors -- at least 8
+    // bound: the 8th smallest of the rows' three smallest errors -- at least 8
     // candidates lie at or below it. Each lane's list is sorted; three
     // bitonic merge stages with the lanes 1, 2 and 4 apart leave every lane
     // with the group's 8 smallest, sorted.
