@@ -221,17 +221,41 @@ __device__ __forceinline__ void scan_chunk(const Region& reg, const float* cur_s
     }
     // merge the rows' three smallest into the lane's 8 smallest (three per
     // row bound the 8th smallest tighter than two, so fewer candidates pass
-    // the selection's bound; a fourth costs more than it saves)
+    // the selection's bound; a fourth costs more than it saves): a bitonic
+    // sorting network over the 3K values, then one bitonic merge with lb --
+    // a few parallel stages instead of a dependent chain of insertions
+    constexpr int N = 3 * K > 8 ? 16 : 8;
+    float v[N];
 #pragma unroll
-    for (int q = 0; q < 3 * K; ++q) {
-        float c = q < K ? m1[q] : (q < 2 * K ? m2[q - K] : m3[q - 2 * K]);
+    for (int i = 0; i < N; ++i)
+        v[i] = i < K ? m1[i] : (i < 2 * K ? m2[i - K] : (i < 3 * K ? m3[i - 2 * K] : kFltMax));
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            const float lo = fminf(lb[i], c);
-            c = fmaxf(lb[i], c);
-            lb[i] = lo;
-        }
-    }
+    for (int k = 2; k <= N; k <<= 1)
+#pragma unroll
+        for (int jj = k >> 1; jj > 0; jj >>= 1)
+#pragma unroll
+            for (int i = 0; i < N; ++i) {
+                const int l = i ^ jj;
+                if (l > i) {
+                    const float a = v[i], b = v[l];
+                    const bool up = (i & k) == 0;
+                    v[i] = up ? fminf(a, b) : fmaxf(a, b);
+                    v[l] = up ? fmaxf(a, b) : fminf(a, b);
+                }
+            }
+    // the 8 smallest of both ascending lists form a bitonic sequence ...
+#pragma unroll
+    for (int i = 0; i < 8; ++i) lb[i] = fminf(lb[i], v[7 - i]);
+    // ... which three compare-exchange levels sort
+#pragma unroll
+    for (int dd = 4; dd > 0; dd >>= 1)
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+            if ((i & dd) == 0) {
+                const float a = lb[i], b = lb[i + dd];
+                lb[i] = fminf(a, b);
+                lb[i + dd] = fmaxf(a, b);
+            }
 }
 
 // Exact scan (radius >= 3, src/bm3d.comp:512-526): candidate cx (relative
