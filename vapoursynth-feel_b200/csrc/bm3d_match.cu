@@ -64,6 +64,10 @@ int tile_count(const StackJob& job, TileShape shape) {
 bool tile_shape_fits(const StackJob& job, TileShape shape, TileMode mode) {
     if (job.radius >= 3 && mode != kTableOnly) return false;  // exact scan: table mode only
     if (plan_bytes(job, shape, mode) > kSmemBudget) return false;
+    // scan indices must stay below 2^21 (the kernels' div_small); the
+    // shared-memory plan already keeps them far below
+    const int64_t ws = 2 * (int64_t)job.bm_range + 1, wt = 2 * (int64_t)job.ps_range + 1;
+    if (ws * ws >= (int64_t(1) << 21) || job.ps_num * wt * wt >= (int64_t(1) << 21)) return false;
     if (job.radius > 0) {
         const int cw = std::min(job.bm_range, job.width - 8) + 1;
         const int ch = std::min(job.bm_range, job.height - 8) + 1;

@@ -66,6 +66,23 @@ __device__ __forceinline__ uint64_t make_key(float err, int seq) {
 
 __device__ __forceinline__ float key_err(uint64_t k) { return __uint_as_float(uint32_t(k >> 32)); }
 
+// floor(f / d) for 0 <= f < 2^21 and 1 <= d < 2^24, exactly: (f + 0.5)
+// times the correctly rounded reciprocal of d, truncated. The relative
+// error stays below 2^-23, less than the distance 0.5 / (f + 0.5) from
+// (f + 0.5) / d to an integer, so the truncation is the integer quotient.
+// The tiled kernels divide table indices and scan indices, which stay below
+// 2^21 (tile_shape_fits sends larger windows to the direct-read kernel).
+__device__ __forceinline__ int div_small(int f, int d) {
+    return (int)__fmul_rn(__fadd_rn((float)f, 0.5f), __frcp_rn((float)d));
+}
+
+// the sliding kernel divides with div_small; the exact kernel (whose few
+// divisions sit off its critical path) keeps the integer division
+template <bool kExact>
+__device__ __forceinline__ int qdiv(int f, int d) {
+    return kExact ? f / d : div_small(f, d);
+}
+
 __device__ __forceinline__ int warp_max(int v) {
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) v = max(v, __shfl_xor_sync(kFull, v, off));
@@ -526,7 +543,7 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
                     const int b = __ffs(m) - 1;
                     m &= m - 1;
                     const int f = 4 * (v0 + sub + 8 * (b >> 2)) + (b & 3);
-                    const int d = f / w.h;
+                    const int d = div_small(f, w.h);
                     const int row = f - d * w.h;
                     gs->buf[pos++] = make_key(E[w.eoff + f], w.seq_base + row * w.rw + d);
                 }
@@ -570,7 +587,7 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
                     for (int u = 0; u < 4; ++u) {
                         const int f = 4 * (v0 + sub + 8 * k) + u;
                         if (f < n_w && ev[u] <= terr && ev[u] < kFltMax) {
-                            const int d = f / w.h;
+                            const int d = div_small(f, w.h);
                             const int row = f - d * w.h;
                             const uint32_t seq = uint32_t(w.seq_base + row * w.rw + d);
                             if (ev[u] < terr || seq <= tseq) {
@@ -642,7 +659,7 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
         K = warp_max(rows_per_lane(total_rows));
     }
     int ntasks = 0;
-    for (int i = 0; i < nwin; ++i) ntasks += (wins[i].h + K - 1) / K;
+    for (int i = 0; i < nwin; ++i) ntasks += qdiv<kExact>(wins[i].h + K - 1, K);
     const int rounds = warp_max((ntasks + 7) / 8);
     float lb[8];
     uint64_t top[8];
@@ -655,8 +672,8 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
         const int task = round * 8 + sub;
         const bool has = task < ntasks;
         int wi = 0, c = has ? task : 0;
-        while (wi < nwin - 1 && c >= (wins[wi].h + K - 1) / K) {
-            c -= (wins[wi].h + K - 1) / K;
+        while (wi < nwin - 1 && c >= qdiv<kExact>(wins[wi].h + K - 1, K)) {
+            c -= qdiv<kExact>(wins[wi].h + K - 1, K);
             ++wi;
         }
         Window win = wins[wi];
@@ -696,13 +713,14 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
 }
 
 // Position of a key. Sentinels decode to (0, 0) as in the reference.
+template <bool kExact>
 __device__ __forceinline__ uint32_t key_xy(uint64_t key, const Window* wins, int area) {
     if (key == kKeyMax) return 0u;
     const int seq = int(uint32_t(key));
-    const int wi = area > 0 ? seq / area : 0;
+    const int wi = area > 0 ? qdiv<kExact>(seq, area) : 0;
     const Window w = wins[wi];
     const int rem = seq - w.seq_base;
-    const int dy = rem / w.rw;
+    const int dy = qdiv<kExact>(rem, w.rw);
     const int dx = rem - dy * w.rw;
     return uint32_t(w.left + dx) | (uint32_t(w.top + dy) << 16);
 }
@@ -884,7 +902,7 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         __syncwarp(gmask);
         search_windows<kExact>(s, cur_s, c7, win, 1, E, gs, gmask, job.status);
         const uint64_t k = gs->top[sub];
-        const uint32_t xy = key_xy(k, win, 0);
+        const uint32_t xy = key_xy<kExact>(k, win, 0);
         // the global match list: lane `sub` holds entry sub
         ge = key_err(k);
         gxy = xy;
@@ -917,7 +935,7 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
             // parallel
             for (int i = 0; i < P; ++i) {
                 const uint64_t k = gs->top[i];
-                const uint32_t fxy = key_xy(k, win, area);
+                const uint32_t fxy = key_xy<kExact>(k, win, area);
                 const float err = key_err(k);
                 const float e7 = __shfl_sync(gmask, ge, 7, 8);
                 const unsigned below = __ballot_sync(gmask, ge <= err);
