@@ -166,6 +166,21 @@ def test_error_against_the_fp64_oracle(oracle_lib):
     assert np.mean(d > 1e-4) < 1e-3
 
 
+def test_overlapped_and_serial_schedules_agree(monkeypatch):
+    """Filtering beside the next stack's matching (the default) against one
+    stream (VSFEEL_OVERLAP_FILTER=0): the same work, reordered; with the
+    extractor every addend is exact, so those outputs are bit-identical."""
+    frames = make_clip(9, 72, 96, sigma=5.0, seed=31)
+    for kw, tol in ((dict(sigma=5.0, block_step=4, bm_range=10, radius=2, ps_num=2, ps_range=4),
+                     TYPICAL_TOL),
+                    (dict(sigma=5.0, block_step=3, bm_range=8, radius=1, extractor_exp=2), 0.0)):
+        monkeypatch.setenv("VSFEEL_OVERLAP_FILTER", "1")
+        a = _node(frames, **kw).output()
+        monkeypatch.setenv("VSFEEL_OVERLAP_FILTER", "0")
+        b = _node(frames, **kw).output()
+        assert np.abs(a - b).max() <= tol, kw
+
+
 def test_get_frame_matches_whole_clip():
     frames = make_clip(9, 72, 96, sigma=5.0, seed=3)
     node = _node(frames, sigma=5.0, block_step=4, bm_range=10, radius=2, ps_num=2, ps_range=4)
