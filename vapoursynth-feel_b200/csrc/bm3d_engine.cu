@@ -656,6 +656,20 @@ struct vsfeel_bm3d {
             VSF_CUDA(cudaStreamWaitEvent(fs, ev_fork, 0));
             VSF_CUDA(cudaStreamWaitEvent(ms, ev_fork, 0));
         }
+        // st waits for both streams on every exit, an error's included, so
+        // that no later call's work overlaps this call's
+        struct Join {
+            vsfeel_bm3d* c;
+            bool on;
+            cudaStream_t st, fs, ms;
+            ~Join() {
+                if (!on) return;
+                cudaEventRecord(c->ev_join, fs);
+                cudaStreamWaitEvent(st, c->ev_join, 0);
+                cudaEventRecord(c->ev_join_match, ms);
+                cudaStreamWaitEvent(st, c->ev_join_match, 0);
+            }
+        } join{this, two, st, fs, ms};
         for (int m = m_lo; m <= m_hi; ++m) {
             const int want = std::min(last, m + r);
             if (!two) {
@@ -690,12 +704,6 @@ struct vsfeel_bm3d {
                 if (after_output) (*after_output)(n, fs);
             }
             finished = std::max(finished, done);
-        }
-        if (two) {
-            VSF_CUDA(cudaEventRecord(ev_join, fs));
-            VSF_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
-            VSF_CUDA(cudaEventRecord(ev_join_match, ms));
-            VSF_CUDA(cudaStreamWaitEvent(st, ev_join_match, 0));
         }
     }
 
