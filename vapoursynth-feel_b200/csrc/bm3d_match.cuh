@@ -5,15 +5,17 @@
 // four blocks of one block row, two block columns apart. For each search
 // phase (the spatial window in frame m, then one temporal step per frame) the
 // CTA stages the frame region that every window of the tile can reach
-// (tile +- bm_range + t*ps_range) in shared memory once, column-major.
+// (tile +- bm_range + t*ps_range) in shared memory once (cp.async),
+// row-major (the exact scan for radius >= 3 stages it column-major).
 //
 // Scan. Within a block, lane s takes a chunk of K consecutive candidate rows
-// of a window and sweeps the window's columns left to right. One step loads
-// the K+7 source values of column X (consecutive words), updates the K
-// column sums
+// of a window and sweeps the window's columns left to right, two columns
+// per iteration: the K+7 source rows of columns X, X+1 are K+7 8-byte pairs,
+// and the column sums
 //     V(X) = SSD(source column X, block column min(X - left, 7))
-// and advances, per row, the reduction tree of the reference in incremental
-// form: P(j) = V(j) + V(j+1), Q(j) = P(j) + P(j+2), E(j) = Q(j) + Q(j+4) --
+// of X and X+1 run in the two halves of f32x2 registers. Per row the
+// reduction tree of the reference advances in incremental form:
+// P(j) = V(j) + V(j+1), Q(j) = P(j) + P(j+2), E(j) = Q(j) + Q(j+4) --
 // the same additions on the same operands as
 // ((c0+c1)+(c2+c3))+((c4+c5)+(c6+c7)), so every candidate error carries the
 // reference's bits. Every error is stored to the block's error table in
