@@ -338,10 +338,11 @@ __device__ __forceinline__ void scan_chunk_exact(const Region& reg, const float*
     const int seq0 = win.seq_base + (r0 - win.top) * win.rw;
     const u64* bpair = reinterpret_cast<const u64*>(cur_p);
 
-    for (int j0 = 0; j0 < jcount; j0 += 4) {
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            const int j = j0 + u;
+    // step j (ring positions u = j mod 4); in the first four steps (head)
+    // the pairs with cp > j feed no candidate (S_c belongs to candidate
+    // j - c < 0) and are skipped -- statically, as those steps are peeled
+    auto step = [&](const int j, const int u, const bool head) {
+        {
             u64 wd[K + 7];  // source values, each in both halves
             {
                 const float* col = sbase + min(win.left + j, xmax) * cs;
@@ -351,6 +352,11 @@ __device__ __forceinline__ void scan_chunk_exact(const Region& reg, const float*
             u64 S[K][4];  // {S_cp, S_cp+4}
 #pragma unroll
             for (int cp = 0; cp < 4; ++cp) {
+                if (head && cp > u) {
+#pragma unroll
+                    for (int q = 0; q < K; ++q) S[q][cp] = 0ull;
+                    continue;
+                }
                 u64 b[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) b[i] = bpair[8 * cp + i];
@@ -392,6 +398,12 @@ __device__ __forceinline__ void scan_chunk_exact(const Region& reg, const float*
                         insert_key(top, make_key(e[q], seq0 + q * win.rw + d));
             }
         }
+    };
+#pragma unroll
+    for (int u = 0; u < 4; ++u) step(u, u, true);
+    for (int j0 = 4; j0 < jcount; j0 += 4) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) step(j0 + u, u, false);
     }
 }
 
