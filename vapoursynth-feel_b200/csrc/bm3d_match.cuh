@@ -401,9 +401,12 @@ __device__ __forceinline__ void scan_chunk_exact(const Region& reg, const float*
     };
 #pragma unroll
     for (int u = 0; u < 4; ++u) step(u, u, true);
+    // steps past jcount (the rest of the last group of four) would only feed
+    // candidates right of every window of the warp: skipped (warp-uniform)
     for (int j0 = 4; j0 < jcount; j0 += 4) {
 #pragma unroll
-        for (int u = 0; u < 4; ++u) step(j0 + u, u, false);
+        for (int u = 0; u < 4; ++u)
+            if (j0 + u < jcount) step(j0 + u, u, false);
     }
 }
 
