@@ -37,7 +37,11 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_SRC = Path("/root/reference/src")
+# The reference tree's shader directory: VSFEEL_REFERENCE_SRC, or the
+# ``--reference-src DIR`` argument of ``python -m oracle.build``, else the
+# path where the reference is checked out beside this repository's builds.
+DEFAULT_REF_SRC = Path("/root/reference/src")
+REF_SRC = Path(os.environ.get("VSFEEL_REFERENCE_SRC", str(DEFAULT_REF_SRC)))
 REF_OUT = HERE / "_ref"
 ORACLE_SO = HERE / "libbm3d_oracle.so"
 REF_SO = REF_OUT / "libvsfeel_ref.so"
@@ -142,16 +146,19 @@ extern "C" void {namespace}_entry() {{ {namespace}::shader_main(); }}
 """
 
 
-def reference_available() -> bool:
-    return (REF_SRC / "bm3d.comp").is_file() and (REF_SRC / "bm3d_agg.comp").is_file()
+def reference_available(src: Path | None = None) -> bool:
+    src = Path(src) if src else REF_SRC
+    return (src / "bm3d.comp").is_file() and (src / "bm3d_agg.comp").is_file()
 
 
-def build_ref(force: bool = False) -> Path | None:
-    """Compiles the reference shaders for the CPU; None when the tree is absent."""
-    if not reference_available():
+def build_ref(force: bool = False, src: str | os.PathLike | None = None) -> Path | None:
+    """Compiles the reference shaders under ``src`` (default REF_SRC) for the
+    CPU; None when the tree is absent and nothing was built before."""
+    src = Path(src) if src else REF_SRC
+    if not reference_available(src):
         return REF_SO if REF_SO.exists() else None
     REF_OUT.mkdir(exist_ok=True)
-    shaders = {"ref_bm3d": REF_SRC / "bm3d.comp", "ref_bm3d_agg": REF_SRC / "bm3d_agg.comp"}
+    shaders = {"ref_bm3d": src / "bm3d.comp", "ref_bm3d_agg": src / "bm3d_agg.comp"}
     harness = HERE / "ref_harness.cpp"
     simt_h = HERE / "ref_simt.h"
     deps = [*shaders.values(), harness, simt_h, Path(__file__)]
@@ -172,10 +179,17 @@ def build_ref(force: bool = False) -> Path | None:
     return REF_SO
 
 
-def main() -> int:
-    force = "--force" in sys.argv
-    print(build_oracle(force))
-    print(build_ref(force))
+def main(argv: list[str] | None = None) -> int:
+    import argparse
+
+    ap = argparse.ArgumentParser(description="build the CPU checkers")
+    ap.add_argument("--force", action="store_true", help="rebuild even when up to date")
+    ap.add_argument("--reference-src", default=None,
+                    help="the reference tree's src/ directory (default: VSFEEL_REFERENCE_SRC "
+                         f"or {DEFAULT_REF_SRC})")
+    a = ap.parse_args(argv)
+    print(build_oracle(a.force))
+    print(build_ref(a.force, a.reference_src))
     return 0
 
 

@@ -18,8 +18,9 @@ PKG_FILES = ("vsfeel/__init__.py", "vsfeel/_lib.py", "vsfeel/autograd.py", "vsfe
              "vsfeel/include/vsfeel_bm3d.h")
 
 
-@pytest.fixture(scope="module")
-def wheel(tmp_path_factory):
+def _build_wheel(tmp_path_factory, env=None):
+    import os
+
     lib = ROOT / "vapoursynth-feel_b200" / "vsfeel" / "libvsfeel_bm3d.so"
     if not lib.exists():
         pytest.skip("library not built")
@@ -32,10 +33,29 @@ def wheel(tmp_path_factory):
                     ignore=shutil.ignore_patterns("__pycache__", "*.o"))
     out = tmp_path_factory.mktemp("dist")
     subprocess.run([sys.executable, "-m", "pip", "wheel", "--no-deps", "--no-build-isolation",
-                    "--no-index", "-q", "-w", str(out), str(src)], check=True, timeout=600)
+                    "--no-index", "-q", "-w", str(out), str(src)], check=True, timeout=600,
+                   env={**os.environ, **(env or {})})
     wheels = list(out.glob("*.whl"))
     assert len(wheels) == 1, wheels
     return wheels[0]
+
+
+@pytest.fixture(scope="module")
+def wheel(tmp_path_factory):
+    return _build_wheel(tmp_path_factory, {"VSFEEL_VS_PLUGIN": ""})
+
+
+@pytest.fixture(scope="module")
+def plugin_wheel(tmp_path_factory):
+    """A wheel built with a VapourSynth plugin supplied from outside (the SDK
+    header is not installed here, so a stand-in shared object plays the
+    plugin: only its placement is under test)."""
+    d = tmp_path_factory.mktemp("plugin")
+    c = d / "stand_in.c"
+    c.write_text("int vsfeel_plugin_stand_in(void) { return 7; }\n")
+    so = d / "stand_in.so"
+    subprocess.run(["gcc", "-shared", "-fPIC", str(c), "-o", str(so)], check=True, timeout=120)
+    return _build_wheel(tmp_path_factory, {"VSFEEL_VS_PLUGIN": str(so)}), so
 
 
 def test_wheel_contents_and_tag(wheel):
@@ -72,3 +92,43 @@ def test_installed_wheel_loads_the_library(wheel, tmp_path):
                          text=True, cwd=tmp_path, timeout=120)
     assert res.returncode == 0, res.stderr
     assert res.stdout.strip() == "1"
+
+
+def test_wheel_places_the_vapoursynth_plugin_where_vapoursynth_autoloads(plugin_wheel):
+    wheel, so = plugin_wheel
+    with zipfile.ZipFile(wheel) as z:
+        names = set(z.namelist())
+        # the reference's wheel layout (hatch_build.py:12-24): the plugin in
+        # vapoursynth/plugins/vsfeel of site-packages, the library beside the
+        # package (the plugin's run path: $ORIGIN/../../../vsfeel)
+        assert "vapoursynth/plugins/vsfeel/libvsfeel.so" in names
+        assert "vsfeel/libvsfeel_bm3d.so" in names
+        assert z.read("vapoursynth/plugins/vsfeel/libvsfeel.so") == so.read_bytes()
+
+
+def test_wheel_without_sdk_ships_no_plugin(wheel):
+    with zipfile.ZipFile(wheel) as z:
+        assert not any(n.startswith("vapoursynth/") for n in z.namelist())
+
+
+def test_vapoursynth_shim_registers_the_reference_interface():
+    """The shim source (compiled only where VapourSynth4.h is installed)
+    registers BM3Dv2 in the reference's namespace with its argument string
+    byte for byte (src/bm3d.cpp:1562-1571, src/vsfeel.cpp:350-364) and
+    forwards to the C ABI."""
+    import re
+
+    src = (ROOT / "vapoursynth-feel_b200" / "csrc" / "vs_shim.cpp").read_text()
+    assert "VS_EXTERNAL_API(void) VapourSynthPluginInit2(" in src
+    assert '"com.thefeeltrain.vsfeel", "vsfeel"' in src
+    reg = src[src.index('registerFunction("BM3Dv2"'):]
+    reg = reg[:reg.index("bm3d_create")]
+    joined = "".join(re.findall(r'"([^"]*)"', reg))
+    assert joined == ("BM3Dv2"
+                      "clip:vnode;ref:vnode:opt;sigma:float[]:opt;block_step:int[]:opt;"
+                      "bm_range:int[]:opt;radius:int:opt;ps_num:int[]:opt;ps_range:int[]:opt;"
+                      "num_streams:int:opt;extractor_exp:int:opt;"
+                      "clip:vnode;")
+    for call in ("vsfeel_bm3d_create(", "vsfeel_bm3d_frame_range(", "vsfeel_bm3d_get_frame(",
+                 "vsfeel_bm3d_get_frame_ref(", "vsfeel_bm3d_free("):
+        assert call in src, call

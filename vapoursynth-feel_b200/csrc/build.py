@@ -71,5 +71,55 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
+# The VapourSynth plugin (vs_shim.cpp): built only where the SDK header
+# VapourSynth4.h is installed; the SDK is not part of this repository.
+SHIM_SRC = CSRC / "vs_shim.cpp"
+SHIM_LIB = CSRC / "_build" / "libvsfeel.so"
+
+
+def vapoursynth_include() -> Path | None:
+    """The directory holding VapourSynth4.h: $VAPOURSYNTH_INCLUDE, pkg-config's
+    vapoursynth flags, or the usual system locations; None when absent."""
+    cands = []
+    if os.environ.get("VAPOURSYNTH_INCLUDE"):
+        cands.append(Path(os.environ["VAPOURSYNTH_INCLUDE"]))
+    try:
+        out = subprocess.run(["pkg-config", "--cflags-only-I", "vapoursynth"],
+                             capture_output=True, text=True, timeout=10)
+        if out.returncode == 0:
+            cands += [Path(f[2:]) for f in out.stdout.split() if f.startswith("-I")]
+    except (OSError, subprocess.TimeoutExpired):
+        pass
+    cands += [Path("/usr/include/vapoursynth"), Path("/usr/local/include/vapoursynth")]
+    for c in cands:
+        if (c / "VapourSynth4.h").is_file():
+            return c
+    return None
+
+
+def build_vs_shim(force: bool = False) -> Path | None:
+    """Compiles the VapourSynth plugin against libvsfeel_bm3d.so; None when
+    the SDK header is not installed. Its run path finds the library in the
+    installed layout (site-packages/vapoursynth/plugins/vsfeel/ ->
+    site-packages/vsfeel/) and beside itself."""
+    inc = vapoursynth_include()
+    if inc is None:
+        return None
+    lib = build()
+    if not force and SHIM_LIB.exists() and SHIM_LIB.stat().st_mtime > max(
+            SHIM_SRC.stat().st_mtime, lib.stat().st_mtime):
+        return SHIM_LIB
+    SHIM_LIB.parent.mkdir(exist_ok=True)
+    cxx = os.environ.get("CXX", "g++")
+    cmd = [cxx, "-std=c++17", "-O2", "-fPIC", "-shared", "-fvisibility=hidden", "-I", str(inc),
+           "-I", str(INCLUDE), str(SHIM_SRC), "-L", str(PKG), "-lvsfeel_bm3d",
+           "-Wl,-rpath,$ORIGIN/../../../vsfeel", "-Wl,-rpath,$ORIGIN", "-o", str(SHIM_LIB)]
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        raise RuntimeError(f"VapourSynth plugin build failed:\n{proc.stdout}\n{proc.stderr}")
+    return SHIM_LIB
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))
+    print(build_vs_shim(force="--force" in sys.argv) or "VapourSynth4.h not found: plugin skipped")
