@@ -20,8 +20,11 @@ reference benchmark's BM3D settings (benchmark/bench.py:108-121,167-180).
 (oracle/_ref) on the same workload instead; N>1 ranks other than 0 exit.
 
 Usage: python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-For N > 1 launch one process per GPU with torch.distributed.run; every rank
-denoises its own clip (weak scaling, no collective on the data path).
+For N > 1 launch one process per GPU with torch.distributed.run. The ranks
+shard one clip of 32*N frames with vsfeel.shard.plan: each denoises its 32
+output frames from its sub-clip, which carries a 2r-frame halo on each
+interior side, and computes the halo's extra stacks itself (weak scaling:
+32 output frames per GPU; no collective on the data path).
 """
 
 from __future__ import annotations
@@ -66,15 +69,60 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _profile_traffic():
-    """dram bytes per launch of the match kernel from the committed ncu summary."""
+def _profile_value(prefix: str):
+    """The first number after `prefix` on a line of the committed ncu summary
+    of the match kernel, or None."""
     try:
         for line in PROFILE_FILE.read_text().splitlines():
-            if line.startswith("dram_bytes_per_launch_full_size:"):
-                return int(float(line.split(":", 1)[1].split()[0]))
+            if line.startswith(prefix):
+                return float(line[len(prefix):].replace(":", " ").split()[0])
     except Exception:
         pass
     return None
+
+
+def _profile_traffic():
+    """dram bytes per launch of the match kernel from the committed ncu summary."""
+    v = _profile_value("dram_bytes_per_launch_full_size")
+    return int(v) if v is not None else None
+
+
+# Useful FP32 work of the radius < 3 search, in the reference's sliding-column
+# form (src/bm3d.comp:497-511): per candidate one new column SSD (8
+# subtractions and 8 fused multiply-adds, 24 flops) and the three additions
+# that advance the 8-column tree.
+FLOPS_PER_CANDIDATE = 27
+
+
+def candidates_per_stack(width: int, height: int, p: dict) -> int:
+    """Candidates one stack evaluates: each block's spatial window clamped to
+    the frame, plus 2r * ps_num temporal windows of (2Q+1)^2, clamped as if
+    centred on the block itself (the predictors are matches near it)."""
+    import numpy as np
+
+    step = p["block_step"]
+
+    def widths(extent, reach):
+        nb = (extent - 9 + 2 * step) // step
+        pos = np.minimum(np.arange(nb) * step, extent - 8)
+        return np.minimum(pos + reach, extent - 8) - np.maximum(pos - reach, 0) + 1
+
+    spatial = int(widths(width, p["bm_range"]).sum()) * int(widths(height, p["bm_range"]).sum())
+    temporal = int(widths(width, p["ps_range"]).sum()) * int(widths(height, p["ps_range"]).sum())
+    return spatial + 2 * p["radius"] * p["ps_num"] * temporal
+
+
+def fp32_peak_tflops(torch, dev) -> tuple[float, str]:
+    """FP32 CUDA-core peak: SMs x 128 lanes x 2 flops (FMA) x the max SM clock
+    (MEASURED_PEAKS.json's sm_max_mhz, else 1965 MHz)."""
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz, src = 1965.0, "nominal max SM clock"
+    try:
+        mhz = float(json.loads((ROOT / "MEASURED_PEAKS.json").read_text())["sm_max_mhz"])
+        src = "MEASURED_PEAKS.json sm_max_mhz"
+    except Exception:
+        pass
+    return sms * 128 * 2 * mhz * 1e6 / 1e12, f"{sms} SMs x 128 FP32 lanes x 2 flop x {mhz:.0f} MHz ({src})"
 
 
 class ClockSampler:
@@ -383,8 +431,15 @@ def run_reference(args) -> int:
         kind = "reference"
 
         def step(rows):
-            ref.stack_rows(luma, p, 2, (nby - rows) // 2, rows, nthreads=threads)
-        what = "reference shaders (src/bm3d.comp) compiled for the CPU"
+            # four bands spread from the top edge to the bottom edge, so that
+            # edge rows (clamped, cheaper windows) are sampled in proportion
+            bands = min(4, rows)
+            for k in range(bands):
+                n = rows // bands + (1 if k < rows % bands else 0)
+                first = (nby - n) * k // max(bands - 1, 1)
+                ref.stack_rows(luma, p, 2, first, n, nthreads=threads)
+        what = ("reference shaders (src/bm3d.comp) compiled for the CPU, rows in four bands "
+                "from the top edge to the bottom edge")
     else:
         o = Oracle()
         kind = "port"
@@ -459,7 +514,7 @@ def main() -> int:
     import torch.distributed as dist
 
     import vsfeel
-    from vsfeel.synthetic import make_chroma, make_clip
+    from vsfeel.synthetic import make_chroma, make_clip_range
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -482,17 +537,39 @@ def main() -> int:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    # one clip of nfr frames per rank, sharded by output range: this rank
+    # denoises outputs out_first.. of the whole clip from its sub-clip
+    # (its range plus the 2r-frame halo), generated alone
+    from vsfeel import shard as shard_mod
+
     nfr = args.frames
-    luma = make_clip(nfr, HEIGHT, WIDTH, sigma=3.0, shift=4, seed=2000 + rank)
-    u = make_chroma(nfr, HEIGHT // 2, WIDTH // 2, seed=2000 + rank)
-    v = make_chroma(nfr, HEIGHT // 2, WIDTH // 2, seed=3000 + rank)
+    total_frames = nfr * world
+    shards = shard_mod.plan(total_frames, world, PARAMS["radius"])
+    sh = shards[rank]
+    luma = make_clip_range(total_frames, sh.in_first, sh.in_count, HEIGHT, WIDTH, sigma=3.0,
+                           shift=4, seed=2000)
+    u = make_chroma(sh.in_count, HEIGHT // 2, WIDTH // 2, seed=2000 + sh.in_first)
+    v = make_chroma(sh.in_count, HEIGHT // 2, WIDTH // 2, seed=3000 + sh.in_first)
+    r = PARAMS["radius"]
+
+    def stacks_of(s):
+        # stacks a shard computes: its outputs' stacks, clamped to its sub-clip
+        lo = max(s.local_first - r, 0)
+        hi = min(s.local_first + s.out_count - 1 + r, s.in_count - 1)
+        return hi - lo + 1 if s.out_count else 0
+
+    halo_fraction = sum(stacks_of(s) for s in shards) / total_frames - 1.0
 
     # ---- device-resident pass ------------------------------------------------
     node = vsfeel.BM3Dv2(vsfeel.clip_from_array(luma, u, v), device=local_rank, **PARAMS)
     d_src = torch.from_numpy(luma).to(dev)
-    d_out = torch.empty_like(d_src)
+    d_out = torch.empty((sh.out_count, HEIGHT, WIDTH), dtype=torch.float32, device=dev)
+
+    def run_device():
+        node.output_device(d_src, d_out, first=sh.local_first, count=sh.out_count)
+
     for _ in range(args.warmup):
-        node.output_device(d_src, d_out)
+        run_device()
     torch.cuda.synchronize()
     barrier()
     clocks = ClockSampler(_device_id(torch, dev))
@@ -505,7 +582,7 @@ def main() -> int:
     torch.cuda.synchronize()
     start.record()
     for _ in range(args.steps):
-        node.output_device(d_src, d_out)
+        run_device()
     stop.record()
     torch.cuda.synchronize()
     elapsed_ms = start.elapsed_time(stop)
@@ -516,27 +593,28 @@ def main() -> int:
     barrier()
     elapsed_ms = max_over_ranks(elapsed_ms)
     ms_per_step = elapsed_ms / args.steps
-    px_per_step = nfr * WIDTH * HEIGHT
-    value = world * px_per_step / (ms_per_step / 1e3) / 1e6
+    px_per_step = total_frames * WIDTH * HEIGHT  # output pixels of all ranks
+    value = px_per_step / (ms_per_step / 1e3) / 1e6
 
     # ---- end to end through the host entry point (pinned buffers) -----------
     e2e = None
     if not args.no_e2e:
         h_src = torch.from_numpy(luma).pin_memory()
-        h_out = torch.empty(luma.shape, dtype=torch.float32).pin_memory()
+        h_out = torch.empty((sh.out_count, HEIGHT, WIDTH), dtype=torch.float32).pin_memory()
         enode = vsfeel.BM3Dv2(vsfeel.clip_from_array(h_src.numpy(), u, v), device=local_rank,
                               **PARAMS)
         out_np = h_out.numpy()
         for _ in range(max(1, args.warmup)):
-            enode.output(out=out_np)
+            enode.output(sh.local_first, sh.out_count, out=out_np)
         barrier()
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            enode.output(out=out_np)
+            enode.output(sh.local_first, sh.out_count, out=out_np)
         e2e_s = max_over_ranks((time.perf_counter() - t0) / args.steps)
-        e2e = {"value": world * px_per_step / e2e_s / 1e6, "unit": UNIT,
+        e2e = {"value": px_per_step / e2e_s / 1e6, "unit": UNIT,
                "h2d_bytes_per_step": int(h_src.numel() * 4),
                "d2h_bytes_per_step": int(h_out.numel() * 4),
+               "bytes_note": "this rank's copies (its sub-clip up, its outputs down)",
                "max_abs_diff_vs_device_path": float(np.abs(out_np - d_out.cpu().numpy()).max())}
 
     # ---- roofline of the dominant kernel ------------------------------------
@@ -546,9 +624,25 @@ def main() -> int:
     achieved = alg_bytes / avg_s / 1e9 if avg_s > 0 else 0.0
     peak, peak_src = _peaks()
     traffic = _profile_traffic()
+    cands = candidates_per_stack(WIDTH, HEIGHT, PARAMS)
+    useful_flops = cands * FLOPS_PER_CANDIDATE
+    fp32_peak, fp32_src = fp32_peak_tflops(torch, dev)
+    fp32_achieved = useful_flops / avg_s / 1e12 if avg_s > 0 else 0.0
+    compute = {"bound": "fp32", "achieved": fp32_achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+               "frac": fp32_achieved / fp32_peak, "peak_source": fp32_src,
+               "useful_flops_per_launch": useful_flops, "candidates_per_launch": cands,
+               "flops_per_candidate": FLOPS_PER_CANDIDATE,
+               "flops_note": "the reference's sliding-column SSD: one new column SSD (24 flops) "
+                             "and 3 tree additions per candidate; warm-up columns, idle lanes "
+                             "and selection are overhead, not counted",
+               "ncu_sm_throughput_pct": _profile_value("sm__throughput (pct of peak)"),
+               "ncu_fma_pipe_pct": _profile_value("sm__pipe_fma_cycles_active (pct of peak)")}
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
                 "kernel": "bm3d_match_kernel", "peak_source": peak_src,
+                "binding_roof": "compute (FP32 CUDA-core issue): see roofline.compute; the HBM "
+                                "fraction is far below it by the algorithm's 8 B/px",
+                "compute": compute,
                 "avg_launch_ms": avg_s * 1e3, "algorithmic_bytes_per_launch": alg_bytes,
                 # summed event spans per kernel kind; filtering and normalisation run
                 # on a second stream beside the matching, so their spans overlap it
@@ -566,8 +660,11 @@ def main() -> int:
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {**CONFIG, "frames_per_step": nfr,
-                   "parallelism": f"frame-shard x{world} (independent clips)"},
+        "config": {**CONFIG, "frames_per_step": total_frames,
+                   "parallelism": f"frame-shard x{world}: one clip of {total_frames} frames, "
+                                  f"{nfr} output frames per rank plus a {2 * r}-frame halo "
+                                  f"per interior side"},
+        "halo_recompute_fraction": halo_fraction,
         "e2e": e2e,
         "gpu_launches": int(launches),
         "roofline": roofline,

@@ -129,7 +129,10 @@ typedef void (*vsfeel_release_fn)(void* user, int n);
  * frames of frame_range(n) only), and computed stacks are cached, so
  * requests in or near order compute each stack once. Calls from several
  * threads may overlap: a call holds the context while it enqueues its work
- * and waits for its own output without it. */
+ * and waits for its own output without it. A frame is released once the
+ * library no longer reads it; if a bounded wait for its upload runs out
+ * (VSFEEL_E_TIMEOUT) the frame is not released, since the copy may still
+ * read it, and stays the caller's to release after vsfeel_bm3d_free. */
 VSFEEL_API int vsfeel_bm3d_get_frame(vsfeel_bm3d* ctx, int n, vsfeel_fetch_fn fetch,
                           vsfeel_release_fn release, void* user, float* dst,
                           ptrdiff_t dst_stride_bytes);
@@ -151,7 +154,11 @@ VSFEEL_API int vsfeel_bm3d_get_frame_ref(vsfeel_bm3d* ctx, int n, vsfeel_fetch2_
 /* Whole clip from host memory: src holds all num_frames luma planes
  * (frame f at src + f*frame_stride_bytes, rows row_stride_bytes apart);
  * writes output frames first .. first+count-1 to dst (same layout, frame 0
- * of dst = output `first`). Pinned host buffers give the fastest copies. */
+ * of dst = output `first`). Pinned host buffers give the fastest copies.
+ * A VSFEEL_E_TIMEOUT return leaves copies from src and into dst queued or
+ * running: both buffers stay in use until a later call on the same context
+ * returns VSFEEL_OK (it runs after all earlier work) or vsfeel_bm3d_free
+ * returns, and must not be freed or reused before then. */
 VSFEEL_API int vsfeel_bm3d_process_host(vsfeel_bm3d* ctx, const float* src, ptrdiff_t src_frame_stride_bytes,
                              ptrdiff_t src_row_stride_bytes, float* dst,
                              ptrdiff_t dst_frame_stride_bytes, ptrdiff_t dst_row_stride_bytes,
@@ -338,11 +345,14 @@ VSFEEL_API void vsfeel_bm3d_batch_free(vsfeel_bm3d_batch* batch);
  * process_device does, and keeps every intermediate in one static device
  * array of vsfeel_bm3d_noalloc_scratch_bytes() (32 MiB), held by every GPU
  * that loads the library until exit; clips whose match table and
- * accumulator planes need more are rejected with an error. The first call
- * on each device resolves the array's device address, so make it before any
- * stream capture. The call only enqueues work on `stream` (used as given)
- * and never waits. All calls share the array: calls that overlap on the GPU
- * race and must be serialised by the caller. */
+ * accumulator planes need more are rejected with an error. The array's
+ * device address belongs to a CUDA context: the first call in each context
+ * (the current one; a host's own driver-API context and a primary context
+ * re-created after cudaDeviceReset each count as new) resolves and caches
+ * it, so make that first call before any stream capture. The call only
+ * enqueues work on `stream` (used as given) and never waits. All calls share
+ * the array: calls that overlap on the GPU race and must be serialised by
+ * the caller. */
 VSFEEL_API int vsfeel_bm3d_process_device_noalloc(const vsfeel_bm3d_args* args,
                                                   const vsfeel_bm3d_video_info* vi,
                                                   const float* src, int64_t src_frame_stride,

@@ -6,7 +6,13 @@
 * a bounded wait that runs out (VSFEEL_TIMEOUT_MS = 1 ms against ~15 ms of
   GPU work, pinned buffers so that the copies do not block the host) ->
   VSFEEL_E_TIMEOUT, after which the context still works once the limit is
-  back to normal.
+  back to normal;
+* the kernels' status word: a test hook (VSFEEL_TEST_PROBE_TILE) makes one
+  tile's staged-region check report a window outside the region. The tile
+  sets the word and skips its scan -- no out-of-range access is made -- and
+  the host must turn the word into VSFEEL_E_CUDA "internal error", through
+  the whole-clip path and the per-frame path, after which the same context
+  denoises correctly again.
 """
 
 from __future__ import annotations
@@ -99,3 +105,20 @@ def test_bounded_wait_times_out_and_the_context_recovers(monkeypatch):
     assert run() == _lib.OK
     ref = vsfeel.BM3Dv2(vsfeel.clip_from_array(frames), **params).output(2, 1)
     assert float(np.abs(out.numpy()[2] - ref[0]).max()) <= 2e-5
+
+
+def test_status_word_reaches_the_caller_and_the_context_recovers(monkeypatch):
+    frames = make_clip(3, 64, 80, sigma=5.0, seed=9)
+    node = vsfeel.BM3Dv2(vsfeel.clip_from_array(frames), **PARAMS)
+    expected = vsfeel.BM3Dv2(vsfeel.clip_from_array(frames), **PARAMS).output()
+    msg = "internal error: a search window left the staged region"
+    monkeypatch.setenv("VSFEEL_TEST_PROBE_TILE", "1")
+    with pytest.raises(vsfeel.Error, match=msg):
+        node.output()
+    with pytest.raises(vsfeel.Error, match=msg):
+        node.get_frame(1)
+    monkeypatch.delenv("VSFEEL_TEST_PROBE_TILE")
+    # the word was cleared when it was reported: the same context is clean
+    assert float(np.abs(node.output() - expected).max()) <= 2e-5
+    fresh = vsfeel.BM3Dv2(vsfeel.clip_from_array(frames), **PARAMS)
+    assert float(np.abs(node.get_frame(2)[0] - fresh.get_frame(2)[0]).max()) <= 2e-5

@@ -110,6 +110,31 @@ def test_fp64_frozen_operator_reproduces_forward(name, n, h, w, params):
     assert float((ref - out.double()).abs().max()) <= tol
 
 
+@pytest.mark.parametrize("name,n,h,w,params", [CASES[0], CASES[4]], ids=["r1_small", "extractor"])
+def test_fused_tiles_record_the_same_state(name, n, h, w, params, monkeypatch):
+    """The fused match-and-filter tiles (VSFEEL_FUSED_FILTER=1, shared-memory
+    accumulation of the reference slice) record keep bits and denominators
+    from which the FP64 frozen operator reproduces their output, and give
+    the plain path's output."""
+    import torch
+
+    monkeypatch.setenv("VSFEEL_FUSED_FILTER", "1")
+    frames, x, den = _setup(n, h, w, seed=74, **params)
+    out, saved = den.forward_saved(x)
+    torch.cuda.synchronize()
+    st = _state(den, saved)
+    dref = st.denominators()
+    den_tol = 1e-6 if not params.get("extractor_exp") else 2e-4
+    assert float(((dref - st.den) / dref).abs().max()) <= den_tol
+    tol = OUT_TOL_FP64 if not params.get("extractor_exp") else 1e-4
+    assert float((st.apply(x.double()) - out.double()).abs().max()) <= tol
+    monkeypatch.delenv("VSFEEL_FUSED_FILTER")
+    plain = torch.empty_like(x)
+    vsfeel.BM3Dv2(vsfeel.clip_from_array(frames), **params).output_device(x, plain)
+    torch.cuda.synchronize()
+    assert float((out - plain).abs().max()) <= 2e-5
+
+
 @pytest.mark.parametrize("name,n,h,w,params", CASES, ids=[c[0] for c in CASES])
 def test_gradient_vs_fp64_reference(name, n, h, w, params):
     import torch

@@ -331,3 +331,60 @@ def test_host_entry_point_with_pinned_buffers_and_mixed_streams():
         part.stride(0) * 4, part.stride(1) * 4, 2, 3)
     assert rc == _lib.OK
     assert float(np.abs(part.numpy() - expected[2:5]).max()) <= TYPICAL_TOL
+
+
+@pytest.mark.parametrize("kw,shape", [
+    (dict(sigma=3.0, block_step=4, bm_range=16, radius=2, ps_num=2, ps_range=7), (5, 270, 480)),
+    (dict(sigma=5.0, block_step=3, bm_range=9, radius=1, ps_num=3, ps_range=4,
+          extractor_exp=2), (4, 100, 132)),
+    (dict(sigma=3.0, block_step=8, bm_range=9, radius=0), (3, 96, 160)),
+    (dict(sigma=6.0, block_step=5, bm_range=7, radius=2, ps_num=2, ps_range=3,
+          extractor_exp=1), (6, 41, 77)),
+])
+def test_fused_tiles_with_shared_memory_accumulator_vs_oracle(kw, shape, monkeypatch,
+                                                              oracle_lib):
+    """Matching and filtering in one tiled launch (VSFEEL_FUSED_FILTER=1):
+    each tile accumulates its reference-frame slice in shared memory and
+    flushes it once. Against the oracle: within the bar, and bit-exact with
+    the extractor (every addend a multiple of ulp(E)); frame edges, clip
+    ends and odd sizes included."""
+    monkeypatch.setenv("VSFEEL_FUSED_FILTER", "1")
+    n, h, w = shape
+    frames = make_clip(n, h, w, sigma=kw["sigma"], shift=4, seed=61)
+    p = Params(**kw)
+    expected = oracle_lib.bm3d(frames, p)
+    out = _node(frames, **kw).output()
+    if kw.get("extractor_exp", 0):
+        assert np.array_equal(out, expected)
+    else:
+        assert float(np.abs(out.astype(np.float64) - expected).max()) <= TYPICAL_TOL
+
+
+@pytest.mark.parametrize("kw,shape", [
+    (dict(sigma=3.0, block_step=4, bm_range=16, radius=2, ps_num=2, ps_range=7), (5, 270, 480)),
+    (dict(sigma=3.0, block_step=8, bm_range=9, radius=0), (3, 96, 160)),
+    (dict(sigma=6.0, block_step=3, bm_range=8, radius=2, ps_num=8, ps_range=9), (5, 80, 96)),
+    (dict(sigma=5.0, block_step=5, bm_range=20, radius=1, ps_num=3, ps_range=4,
+          extractor_exp=2), (3, 61, 93)),
+    (dict(sigma=6.0, block_step=4, bm_range=3, radius=2, ps_num=1, ps_range=1), (5, 40, 48)),
+])
+def test_sixteen_lanes_per_block_vs_oracle(kw, shape, monkeypatch, oracle_lib):
+    """The 512-thread form of the sliding matcher (VSFEEL_MATCH_LANES=16:
+    16 lanes per reference block, at most 3 window rows per lane, the match
+    list mirrored in lanes 8..15): match tables bit-exact against the oracle
+    on every stack shown, outputs within the bar (bit-exact with the
+    extractor)."""
+    monkeypatch.setenv("VSFEEL_MATCH_LANES", "16")
+    n, h, w = shape
+    frames = make_clip(n, h, w, sigma=kw["sigma"], shift=4, seed=62)
+    p = Params(**kw)
+    stacks = sorted({0, n // 2, n - 1})
+    cuda = _cuda_tables(frames, p, stacks)
+    for m in stacks:
+        assert np.array_equal(cuda[m], oracle_lib.matches(frames, p, m)), m
+    expected = oracle_lib.bm3d(frames, p)
+    out = _node(frames, **kw).output()
+    if kw.get("extractor_exp", 0):
+        assert np.array_equal(out, expected)
+    else:
+        assert float(np.abs(out.astype(np.float64) - expected).max()) <= TYPICAL_TOL

@@ -63,6 +63,42 @@ def test_noalloc_matches_allocating_entry_point_twice(kw):
         assert diff <= TOL, diff
 
 
+@pytest.mark.parametrize("first,count,kw", [
+    (2, 2, dict(sigma=5.0, block_step=4, bm_range=12, radius=2, ps_num=2, ps_range=5)),
+    (5, 2, dict(sigma=5.0, block_step=4, bm_range=12, radius=2, ps_num=2, ps_range=5)),
+    (0, 3, dict(sigma=6.0, block_step=4, bm_range=10, radius=3, ps_num=4, ps_range=4)),
+    (3, 4, dict(sigma=8.0, block_step=4, bm_range=16, radius=3, ps_num=4, ps_range=7,
+                extractor_exp=2)),
+])
+def test_noalloc_sub_ranges_and_radius3(first, count, kw):
+    """Output ranges that start inside the clip (dst indexed from n - first,
+    the slot ring starting mid-clip) or end before it does, and the radius-3
+    exact matcher, against the allocating entry point on the same range."""
+    import torch
+
+    lib = _lib.load()
+    frames = make_clip(7, 96, 128, sigma=kw["sigma"], shift=4, seed=32)
+    n, h, w = frames.shape
+    src = torch.from_numpy(frames).cuda()
+    expected = torch.empty((count, h, w), device="cuda")
+    node = vsfeel.BM3Dv2(vsfeel.clip_from_array(frames), **kw)
+    node.output_device(src, expected, first=first, count=count)
+    torch.cuda.synchronize()
+
+    args = _args(**kw)
+    vi = _lib.VideoInfo(w, h, n, _lib.CF_GRAY, _lib.ST_FLOAT, 32, 0, 0)
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        out = torch.full((count, h, w), float("nan"), device="cuda")
+        rc = lib.vsfeel_bm3d_process_device_noalloc(
+            ctypes.byref(args), ctypes.byref(vi), src.data_ptr(), src.stride(0), src.stride(1),
+            out.data_ptr(), out.stride(0), out.stride(1), first, count, stream)
+        assert rc == _lib.OK, _lib.last_error(lib)
+        torch.cuda.synchronize()
+        diff = (out - expected).abs().max().item()
+        assert diff <= TOL, diff
+
+
 def test_noalloc_rejects_clips_beyond_its_scratch():
     import torch
 

@@ -3,9 +3,12 @@
 // counterpart in the reference, whose concurrency is num_streams Vulkan
 // queues working on frames of one clip (src/bm3d.cpp:698-1028).
 //
-// Layout. Every clip keeps, per output frame n, the TW (numerator, weight)
-// plane pairs of its contributing stacks (the plain path's slot, without
-// the ring reuse): all stacks of all clips can then be in flight at once.
+// Layout. Every clip of a chunk keeps, per output frame n, the TW
+// (numerator, weight) plane pairs of its contributing stacks (the plain
+// path's slot, without the ring reuse), so that all stacks of a chunk can be
+// in flight at once. Chunks run one after another (and classes one after
+// another), so every chunk of every class uses the same accumulator buffer
+// and the same match-table buffer, sized for the largest chunk.
 // Shape classes group the clips whose stacks share a tiled-kernel
 // configuration. Per class:
 //   * jobs[]: one StackJob per (clip, stack), largest clips first, with the
@@ -142,7 +145,8 @@ struct Clip {
     vsfeel_bm3d_info info;
     int acc_pitch = 0;
     size_t plane = 0;      // floats per accumulator plane
-    size_t acc_off = 0;    // floats from the class's accumulator base
+    size_t acc_off = 0;    // floats from the shared accumulator base (within its chunk)
+    size_t table_off = 0;  // blocks from the shared match-table base (within its chunk)
     int tw() const { return 2 * info.radius + 1; }
     size_t acc_floats() const { return (size_t)info.num_frames * tw() * 2 * plane; }
 };
@@ -163,8 +167,6 @@ struct Class {
     Dev<int> d_norm_first;
     int norm_tiles = 0;
     int nnorm = 0;
-    Dev<float> acc;
-    Dev<uint32_t> match_xy, match_z;  // match tables (one per stack, or one shared)
     Dev<int> d_filter_first;
     int filter_items = 0;
     Dev<int> counter;
@@ -176,6 +178,7 @@ struct Class {
         size_t acc0, acc_floats;           // accumulator range
     };
     std::vector<Chunk> chunks;
+    std::vector<std::vector<int>> chunk_clips;  // the clips of each chunk, in queue order
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
     cudaGraph_t graph = nullptr;
@@ -192,6 +195,10 @@ struct vsfeel_bm3d_batch {
     Dev<int> status;
     cudaEvent_t start = nullptr;  // recorded after each run's last graph
     int64_t device_bytes = 0;
+    // shared by every chunk of every class (they run one after another)
+    Dev<float> acc;
+    Dev<uint32_t> match_xy, match_z;
+    size_t acc_need = 0, table_need = 0;  // floats / blocks of the largest chunk
 
     ~vsfeel_bm3d_batch() {
         if (start) wait_event(start);
@@ -205,14 +212,14 @@ struct vsfeel_bm3d_batch {
             c.d_tile_first.release();
             c.d_norm.release();
             c.d_norm_first.release();
-            c.acc.release();
-            c.match_xy.release();
-            c.match_z.release();
             c.d_filter_first.release();
             c.counter.release();
         }
         if (start) cudaEventDestroy(start);
         status.release();
+        acc.release();
+        match_xy.release();
+        match_z.release();
     }
 
     // The StackJob of stack m of clip c, scattering into the class's
@@ -294,7 +301,7 @@ int autotune(vsfeel_bm3d_batch* b, Class& cls, const StackJob& sample_in, const 
         for (int rep = 0; rep < 4; ++rep) {
             check(cudaMemsetAsync(counter.p, 0, sizeof(int), cls.stream), "cudaMemsetAsync");
             check(cudaEventRecord(e0, cls.stream), "cudaEventRecord");
-            check(launch_batch_tiles(work, TileShape(s), kTableOnly, smem, grid, cls.stream),
+            check(launch_batch_tiles(work, TileShape(s), kTableOnly, 8, smem, grid, cls.stream),
                   "autotune launch");
             check(cudaEventRecord(e1, cls.stream), "cudaEventRecord");
             if (wait_stream(cls.stream) != VSFEEL_OK)
@@ -312,7 +319,10 @@ int autotune(vsfeel_bm3d_batch* b, Class& cls, const StackJob& sample_in, const 
     return best;
 }
 
-void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
+// Chooses the class's tile shape (autotuning it when asked) and cuts its
+// clips into chunks, recording each chunk's accumulator and match-table
+// needs; nothing is allocated for the class yet.
+void plan_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
     check(cudaStreamCreateWithFlags(&cls.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaEventCreateWithFlags(&cls.done, cudaEventDisableTiming), "cudaEventCreate");
     // largest clips first: the queue's tail is made of small tiles
@@ -321,34 +331,24 @@ void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
         const auto& C = b->clips[c].info;
         return (int64_t)A.width * A.height > (int64_t)C.width * C.height;
     });
-    size_t acc_floats = 0;
-    for (int ci : cls.clips) {
-        Clip& c = b->clips[ci];
-        c.acc_off = acc_floats;
-        acc_floats += (c.acc_floats() + 63) & ~size_t(63);
-    }
-    cls.acc.alloc(acc_floats);
-    b->device_bytes += (int64_t)acc_floats * 4;
 
     // which tile shapes fit every stack of the class
     bool fits[kTileShapes];
     for (int s = 0; s < kTileShapes; ++s) fits[s] = true;
-    size_t max_nblocks = 0;
     for (int ci : cls.clips) {
         const Clip& c = b->clips[ci];
-        const StackJob probe = b->make_job(c, cls.acc.p, 0, true);
+        const StackJob probe = b->make_job(c, nullptr, 0, true);
         // the persistent kernel runs the sliding scan (radius < 3)
         for (int s = 0; s < kTileShapes; ++s)
             fits[s] = fits[s] && c.info.radius < 3 &&
                       tile_shape_fits(probe, TileShape(s), kTableOnly);
-        max_nblocks = std::max(max_nblocks, (size_t)c.info.blocks_x * c.info.blocks_y);
     }
     int shape = -1;
     if (forced >= 0 && forced < kTileShapes && fits[forced]) {
         shape = forced;
     } else if (tune) {
         const Clip& big = b->clips[cls.clips.front()];
-        const StackJob sample = b->make_job(big, cls.acc.p, big.info.num_frames / 2, true);
+        const StackJob sample = b->make_job(big, nullptr, big.info.num_frames / 2, true);
         bool any = false;
         for (int s = 0; s < kTileShapes; ++s) any = any || fits[s];
         if (any) shape = autotune(b, cls, sample, fits);
@@ -362,104 +362,110 @@ void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
     }
     cls.tile_shape = shape;
 
-    // queue of (stack, tile) items and the normalisation list
-    // Jobs and outputs, and chunks of whole clips of at least kChunkTiles
-    // queue items (about 16 waves): a chunk's frames and accumulators are
-    // still in L2 when its filter and normalisation run, while the
-    // persistent launch keeps small clips together.
+    // Chunks of whole clips of at least kChunkTiles queue items (about 16
+    // waves): a chunk's frames and accumulators are still in L2 when its
+    // filter and normalisation run, while the persistent launch keeps small
+    // clips together. Without a tile shape every clip is a chunk of its own
+    // (its stacks run one after another and share one match table).
     const int64_t kChunkTiles = (int64_t)b->sms * 16;
+    std::vector<int> cur;
+    size_t acc = 0, blocks = 0;
+    int64_t tiles = 0;
+    auto close = [&] {
+        cls.chunk_clips.push_back(cur);
+        b->acc_need = std::max(b->acc_need, acc);
+        b->table_need = std::max(b->table_need, blocks);
+        cur.clear();
+        acc = blocks = 0;
+        tiles = 0;
+    };
+    for (int ci : cls.clips) {
+        Clip& c = b->clips[ci];
+        const size_t nb = (size_t)c.info.blocks_x * c.info.blocks_y;
+        c.acc_off = acc;
+        c.table_off = blocks;
+        acc += (c.acc_floats() + 63) & ~size_t(63);
+        blocks += shape >= 0 ? nb * c.info.num_frames : nb;
+        if (shape >= 0)
+            tiles += (int64_t)c.info.num_frames *
+                     tile_count(b->make_job(c, nullptr, 0, true), TileShape(shape));
+        cur.push_back(ci);
+        if (shape < 0 || tiles >= kChunkTiles) close();
+    }
+    if (!cur.empty()) close();
+}
+
+// Builds the class's queue, filter and normalisation lists against the
+// shared accumulators and match tables, uploads them and records the
+// class's graph.
+void finish_class(vsfeel_bm3d_batch* b, Class& cls) {
+    const int shape = cls.tile_shape;
     std::vector<int> first, nfirst, ffirst;  // chunk-relative prefix sums, chunk after chunk
     std::vector<NormalizeJob> norm;
-    Class::Chunk cur{};
-    auto open_chunk = [&](size_t acc0) {
-        cur = Class::Chunk{};
-        cur.job0 = (int)cls.jobs.size();
-        cur.norm0 = (int)norm.size();
-        cur.first_off = (int)first.size();
-        cur.ffirst_off = (int)ffirst.size();
-        cur.nfirst_off = (int)nfirst.size();
-        cur.acc0 = acc0;
+    for (const std::vector<int>& members : cls.chunk_clips) {
+        Class::Chunk ch{};
+        ch.job0 = (int)cls.jobs.size();
+        ch.norm0 = (int)norm.size();
+        ch.first_off = (int)first.size();
+        ch.ffirst_off = (int)ffirst.size();
+        ch.nfirst_off = (int)nfirst.size();
+        ch.acc0 = 0;
         first.push_back(0);
         ffirst.push_back(0);
         nfirst.push_back(0);
-    };
-    auto close_chunk = [&](size_t acc_end) {
-        cur.njobs = (int)cls.jobs.size() - cur.job0;
-        cur.nnorm = (int)norm.size() - cur.norm0;
-        cur.tiles = first.back();
-        cur.filter_items = ffirst.back();
-        cur.norm_tiles = nfirst.back();
-        cur.acc_floats = acc_end - cur.acc0;
-        cls.chunks.push_back(cur);
-    };
-    bool open = false;
-    size_t acc_end = 0;
-    for (int ci : cls.clips) {
-        const Clip& c = b->clips[ci];
-        const int N = c.info.num_frames, r = c.info.radius, tw = c.tw();
-        if (!open) {
-            open_chunk(c.acc_off);
-            open = true;
-        }
-        for (int m = 0; m < N; ++m) {
-            StackJob job = b->make_job(c, cls.acc.p, m, false);
-            if (shape >= 0) {
-                cls.smem = std::max(cls.smem, tile_smem_bytes(job, TileShape(shape), kTableOnly));
-                const int64_t t = (int64_t)first.back() + tile_count(job, TileShape(shape));
-                const int64_t fi = (int64_t)ffirst.back() + filter_items(c.info.blocks_x * c.info.blocks_y);
-                if (t > INT32_MAX || fi > INT32_MAX)
-                    throw Fail{VSFEEL_E_ARG, "batch too large for one launch"};
-                first.push_back((int)t);
-                ffirst.push_back((int)fi);
+        size_t acc_end = 0;
+        for (int ci : members) {
+            const Clip& c = b->clips[ci];
+            const int N = c.info.num_frames, r = c.info.radius, tw = c.tw();
+            const size_t nb = (size_t)c.info.blocks_x * c.info.blocks_y;
+            for (int m = 0; m < N; ++m) {
+                StackJob job = b->make_job(c, b->acc.p, m, false);
+                // every stack of a tiled chunk is in flight at once: a match
+                // table each; the direct-read kernels run stack after stack
+                const size_t toff = c.table_off + (shape >= 0 ? (size_t)m * nb : 0);
+                job.match_xy = b->match_xy.p + toff * 8;
+                job.match_z = b->match_z.p + toff;
+                if (shape >= 0) {
+                    cls.smem = std::max(cls.smem, tile_smem_bytes(job, TileShape(shape), kTableOnly));
+                    const int64_t t = (int64_t)first.back() + tile_count(job, TileShape(shape));
+                    const int64_t fi = (int64_t)ffirst.back() + filter_items((int)nb);
+                    if (t > INT32_MAX || fi > INT32_MAX)
+                        throw Fail{VSFEEL_E_ARG, "batch too large for one launch"};
+                    first.push_back((int)t);
+                    ffirst.push_back((int)fi);
+                }
+                cls.jobs.push_back(job);
             }
-            cls.jobs.push_back(job);
-        }
-        for (int n = 0; n < N; ++n) {
-            NormalizeJob nj{};
-            for (int i = 0; i < tw; ++i) {
-                const int m = clampi(n - r + i, 0, N - 1);
-                nj.num[i] = cls.acc.p + c.acc_off + ((size_t)n * tw + (m - (n - r))) * 2 * c.plane;
+            for (int n = 0; n < N; ++n) {
+                NormalizeJob nj{};
+                for (int i = 0; i < tw; ++i) {
+                    const int m = clampi(n - r + i, 0, N - 1);
+                    nj.num[i] = b->acc.p + c.acc_off + ((size_t)n * tw + (m - (n - r))) * 2 * c.plane;
+                }
+                nj.den_offset = (int64_t)c.plane;
+                nj.tw = tw;
+                nj.width = c.info.width;
+                nj.height = c.info.height;
+                nj.src_pitch = c.acc_pitch;
+                nj.out_pitch = (int)c.desc.dst_row_stride;
+                nj.out = c.desc.dst + (size_t)n * c.desc.dst_frame_stride;
+                norm.push_back(nj);
+                const int64_t nt = (int64_t)nfirst.back() + normalize_tiles(nj.width, nj.height);
+                if (nt > INT32_MAX) throw Fail{VSFEEL_E_ARG, "batch too large for one normalise launch"};
+                nfirst.push_back((int)nt);
             }
-            nj.den_offset = (int64_t)c.plane;
-            nj.tw = tw;
-            nj.width = c.info.width;
-            nj.height = c.info.height;
-            nj.src_pitch = c.acc_pitch;
-            nj.out_pitch = (int)c.desc.dst_row_stride;
-            nj.out = c.desc.dst + (size_t)n * c.desc.dst_frame_stride;
-            norm.push_back(nj);
-            const int64_t nt = (int64_t)nfirst.back() + normalize_tiles(nj.width, nj.height);
-            if (nt > INT32_MAX) throw Fail{VSFEEL_E_ARG, "batch too large for one normalise launch"};
-            nfirst.push_back((int)nt);
+            acc_end = c.acc_off + c.acc_floats();
         }
-        acc_end = c.acc_off + c.acc_floats();
-        if (shape < 0 || first.back() >= kChunkTiles) {
-            close_chunk(acc_end);
-            open = false;
-        }
+        ch.njobs = (int)cls.jobs.size() - ch.job0;
+        ch.nnorm = (int)norm.size() - ch.norm0;
+        ch.tiles = first.back();
+        ch.filter_items = ffirst.back();
+        ch.norm_tiles = nfirst.back();
+        ch.acc_floats = acc_end;
+        cls.chunks.push_back(ch);
     }
-    if (open) close_chunk(acc_end);
     for (const Class::Chunk& ch : cls.chunks) cls.tiles += ch.tiles;
-    if (shape < 0) {
-        // direct-read kernels, stack after stack: one match table suffices
-        cls.match_xy.alloc(max_nblocks * 8);
-        cls.match_z.alloc(max_nblocks);
-        for (StackJob& j : cls.jobs) {
-            j.match_xy = cls.match_xy.p;
-            j.match_z = cls.match_z.p;
-        }
-    } else {
-        // every stack of a chunk is in flight at once: one match table each
-        size_t total = 0;
-        for (const StackJob& j : cls.jobs) total += (size_t)j.nbx * j.nby;
-        cls.match_xy.alloc(total * 8);
-        cls.match_z.alloc(total);
-        size_t off = 0;
-        for (StackJob& j : cls.jobs) {
-            j.match_xy = cls.match_xy.p + off * 8;
-            j.match_z = cls.match_z.p + off;
-            off += (size_t)j.nbx * j.nby;
-        }
+    if (shape >= 0) {
         cls.d_filter_first.upload(ffirst);
         cls.d_tile_first.upload(first);
     }
@@ -468,7 +474,6 @@ void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
     cls.d_norm_first.upload(nfirst);
     cls.nnorm = (int)norm.size();
     cls.counter.alloc(cls.chunks.size());
-    b->device_bytes += (int64_t)(cls.match_xy.n + cls.match_z.n) * 4;
 
     // capture the class's run: per chunk, clear its accumulators, match,
     // filter, normalise
@@ -476,12 +481,12 @@ void build_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
     cudaError_t err = cudaMemsetAsync(cls.counter.p, 0, sizeof(int) * cls.chunks.size(), cls.stream);
     for (size_t k = 0; k < cls.chunks.size() && err == cudaSuccess; ++k) {
         const Class::Chunk& ch = cls.chunks[k];
-        err = cudaMemsetAsync(cls.acc.p + ch.acc0, 0, ch.acc_floats * sizeof(float), cls.stream);
+        err = cudaMemsetAsync(b->acc.p + ch.acc0, 0, ch.acc_floats * sizeof(float), cls.stream);
         if (err == cudaSuccess && shape >= 0) {
             const BatchWork work{cls.d_jobs.p + ch.job0, cls.d_tile_first.p + ch.first_off, ch.njobs,
                                  cls.counter.p + k};
             const int grid = std::min(b->sms, ch.tiles);
-            err = launch_batch_tiles(work, TileShape(shape), kTableOnly, cls.smem, grid, cls.stream);
+            err = launch_batch_tiles(work, TileShape(shape), kTableOnly, 8, cls.smem, grid, cls.stream);
             const FilterBatch fw{cls.d_jobs.p + ch.job0, cls.d_filter_first.p + ch.ffirst_off,
                                  ch.njobs};
             if (err == cudaSuccess) err = launch_filter_batch(fw, ch.filter_items, cls.stream);
@@ -571,7 +576,12 @@ int vsfeel_bm3d_batch_create(const vsfeel_bm3d_batch_clip* clips, int nclips, in
         check(cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming), "cudaEventCreate");
         const int forced = ((flags >> 4) & 15) - 1;
         for (Class& cls : b->classes)
-            build_class(b, cls, (flags & VSFEEL_BATCH_AUTOTUNE) != 0, forced);
+            plan_class(b, cls, (flags & VSFEEL_BATCH_AUTOTUNE) != 0, forced);
+        b->acc.alloc(b->acc_need);
+        b->match_xy.alloc(b->table_need * 8);
+        b->match_z.alloc(b->table_need);
+        b->device_bytes = (int64_t)(b->acc.n + b->match_xy.n + b->match_z.n) * 4;
+        for (Class& cls : b->classes) finish_class(b, cls);
     } catch (const Fail& f) {
         rc = error(f.code, f.msg);
     } catch (const std::bad_alloc&) {
@@ -619,7 +629,7 @@ int vsfeel_bm3d_batch_finish(vsfeel_bm3d_batch* b) {
             rc = error(VSFEEL_E_CUDA, std::string("CUDA error: ") + cudaGetErrorString(e));
         } else if (word != 0) {
             cudaMemset(b->status.p, 0, sizeof(int));
-            rc = error(VSFEEL_E_CUDA, "internal error: a search window left the staged region");
+            rc = error(VSFEEL_E_CUDA, status_text(word));
         }
     }
     if (prev >= 0) cudaSetDevice(prev);

@@ -26,7 +26,8 @@ struct StackJob {
                                        // denoised too, except in the final pass)
     const float* slice_input[kMaxTW];  // final pass: the same frames of the clip denoised
     float* slice_dst[kMaxTW];          // numerator plane of each slice's target; null = dropped
-    int64_t dst_plane;                 // floats from a numerator plane to its weight plane
+    int64_t dst_plane;                 // floats from a numerator plane to its weight-origin
+                                       // plane (each patch's weight at its origin)
     int pitch;                         // floats per frame row (inputs)
     int dst_pitch;                     // floats per accumulator row
     int width, height;
@@ -39,15 +40,21 @@ struct StackJob {
     uint32_t* match_z;                 // [nblocks]: 8 x 4-bit slice index
     uint64_t* mask_out;                // [nblocks][8] keep bits of the filter, or null
     int* status;                       // device word, set nonzero on an internal error
+    int lanes;                         // tiled sliding matcher: lanes per block, 8 (also 0)
+                                       // or 16 (table mode only, 512-thread CTAs)
+    int probe_tile;                    // test hook: 1 + index of a tile whose staged-region
+                                       // check reports a window outside (the tile sets
+                                       // *status and scans nothing); 0 = none
 };
 
 // Per-output normalisation: numerator plane read at aggregation step i.
 // The planes' rows (src_pitch floats) are padded to a multiple of 32 floats
 // and their bases 16-byte aligned: the kernel reads them four floats at a
-// time.
+// time. A pixel's weight is the sum of its 8x8 window of the weight-origin
+// plane.
 struct NormalizeJob {
     const float* num[kMaxTW];
-    int64_t den_offset;  // floats from a numerator plane to its weight plane
+    int64_t den_offset;  // floats from a numerator plane to its weight-origin plane
     int tw, width, height, src_pitch, out_pitch;
     float* out;
     float* den_out;  // summed weights (the frozen denominator), or null
@@ -55,7 +62,7 @@ struct NormalizeJob {
 };
 
 // Many normalisations in one launch: output j covers the items
-// tile_first[j] .. tile_first[j+1]-1, one 128x8-pixel tile each.
+// tile_first[j] .. tile_first[j+1]-1, one 120x8-pixel tile each.
 struct NormalizeBatch {
     const NormalizeJob* jobs;
     const int* tile_first;
@@ -110,8 +117,9 @@ size_t tile_smem_bytes(const StackJob& job, TileShape shape, TileMode mode);
 int tile_count(const StackJob& job, TileShape shape);
 cudaError_t launch_match_tiles(const StackJob& job, TileShape shape, TileMode mode,
                                cudaStream_t stream);
-cudaError_t launch_batch_tiles(const BatchWork& work, TileShape shape, TileMode mode, size_t smem,
-                               int grid, cudaStream_t stream);  // mode: kTableOnly or kFused
+// mode: kTableOnly or kFused; lanes: 8, or 16 with kTableOnly
+cudaError_t launch_batch_tiles(const BatchWork& work, TileShape shape, TileMode mode, int lanes,
+                               size_t smem, int grid, cudaStream_t stream);
 
 // Many stacks' filters in one launch: job j covers the items
 // group_first[j] .. group_first[j+1]-1, 16 groups (blocks) each, with its
@@ -126,7 +134,24 @@ inline int filter_items(int nblocks) { return (nblocks + 15) / 16; }
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream);
 cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream);
 cudaError_t launch_normalize_batch(const NormalizeBatch& work, int total_tiles, cudaStream_t stream);
-inline int normalize_tiles(int width, int height) { return ((width + 127) / 128) * ((height + 7) / 8); }
+// The normaliser's tile: 8 rows (one warp each) of 120 pixels (30 lanes of
+// 4 pixels, the warp's other 2 lanes reading the 8-column halo on the left).
+constexpr int kNormTileW = 120, kNormTileH = 8;
+inline int normalize_tiles(int width, int height) {
+    return ((width + kNormTileW - 1) / kNormTileW) * ((height + kNormTileH - 1) / kNormTileH);
+}
+
+// The kernels' status word: bit 0, a search window left its staged region
+// (the window was not scanned); bit 1, a block's selection did not settle
+// within its pass limit (its error table was not valid).
+inline const char* status_text(int word) {
+    if ((word & 3) == 3)
+        return "internal error: a search window left the staged region; a block selection did "
+               "not converge";
+    if (word & 1) return "internal error: a search window left the staged region";
+    if (word & 2) return "internal error: a block selection did not converge";
+    return "internal error: unknown kernel status";
+}
 
 __host__ __device__ inline int block_count(int extent, int step) {
     return (extent - 9 + 2 * step) / step;  // positions x0 = b*step < extent - 8 + step

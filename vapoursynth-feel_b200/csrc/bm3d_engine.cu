@@ -71,6 +71,15 @@ float sigma_factor(bool final_pass) {
     return f;
 }
 
+// Test hook (VSFEEL_TEST_PROBE_TILE=k): tile k-1 of every stack's tiled
+// matching reports a window outside its staged region, so that the status
+// word's path to the caller can be tested without a real fault. Read per
+// call; unset or 0 means off.
+int probe_tile_from_env() {
+    const char* s = std::getenv("VSFEEL_TEST_PROBE_TILE");
+    return (s && *s) ? std::max(0, std::atoi(s)) : 0;
+}
+
 int64_t timeout_ms() {
     const char* s = std::getenv("VSFEEL_TIMEOUT_MS");
     if (s && *s) {
@@ -287,6 +296,10 @@ struct vsfeel_bm3d {
     // run slower than in the standalone filter kernel (3.18 vs 2.71 + 0.19 ms
     // per 1080p stack on B200).
     bool fused = false;
+    // Lanes per reference block of the tiled sliding matcher (radius < 3):
+    // 8 (256-thread CTAs) or 16 (512-thread CTAs, twice the warps per SM at
+    // the same shared memory). VSFEEL_MATCH_LANES overrides the default.
+    int match_lanes = 8;
 
     DevBuf<float> ring;       // (2r+1) slots x TW x {num, den} planes
     DevBuf<uint32_t> match_xy;
@@ -346,9 +359,19 @@ struct vsfeel_bm3d {
         VSF_CUDA(cudaMemcpy(&word, status.p, sizeof(int), cudaMemcpyDeviceToHost));
         if (word != 0) {
             VSF_CUDA(cudaMemset(status.p, 0, sizeof(int)));
-            return fail(VSFEEL_E_CUDA, "internal error: a search window left the staged region");
+            invalidate_stacks();
+            return fail(VSFEEL_E_CUDA, status_text(word));
         }
         return VSFEEL_OK;
+    }
+    // Forgets every cached stack of the per-frame path: after a kernel
+    // flagged an internal error, a cached stack may hold a skipped scan.
+    void invalidate_stacks() { std::fill(stack_tag.begin(), stack_tag.end(), -1); }
+    // recorded after a direct-path upload: the frame is released once it fires
+    cudaEvent_t direct_copy = nullptr;
+    cudaEvent_t direct_copy_done() {
+        if (!direct_copy) VSF_CUDA(cudaEventCreateWithFlags(&direct_copy, cudaEventDisableTiming));
+        return direct_copy;
     }
     std::map<int, int> frame_slot;  // frame cache of the per-frame path
     std::vector<int> slot_frame;
@@ -533,6 +556,8 @@ struct vsfeel_bm3d {
             job.mask_out = reinterpret_cast<uint64_t*>(rec + L.off_mask);
         }
         job.status = status_word();
+        job.probe_tile = probe_tile_from_env();
+        job.lanes = match_lanes;
         return job;
     }
 
@@ -817,6 +842,7 @@ int vsfeel_bm3d_create_plane(const vsfeel_bm3d_args* args, const vsfeel_bm3d_vid
     ctx->acc_plane = (size_t)s.height * ctx->acc_pitch;
     if (const char* v = std::getenv("VSFEEL_FUSED_FILTER")) ctx->fused = v[0] == '1';
     if (const char* v = std::getenv("VSFEEL_OVERLAP_FILTER")) ctx->overlap = v[0] != '0';
+    if (const char* v = std::getenv("VSFEEL_MATCH_LANES")) ctx->match_lanes = std::atoi(v) == 16 ? 16 : 8;
     DeviceGuard dg(device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
@@ -841,6 +867,7 @@ void vsfeel_bm3d_free(vsfeel_bm3d* ctx) {
                 cudaStreamDestroy(cs);
             }
         if (ctx->tail) cudaEventDestroy(ctx->tail);
+        if (ctx->direct_copy) cudaEventDestroy(ctx->direct_copy);
         for (cudaEvent_t e : {ctx->ev_match[0], ctx->ev_match[1], ctx->ev_filter[0], ctx->ev_filter[1],
                               ctx->ev_fork, ctx->ev_join, ctx->ev_join_match})
             if (e) cudaEventDestroy(e);
@@ -1234,10 +1261,15 @@ int get_frame(vsfeel_bm3d* ctx, int n, bool with_ref,
                             ctx->frames.p + ((size_t)slot_f * planes + clip) * ff,
                             sizeof(float) * ctx->acc_pitch, p, stride, row_bytes, s.height,
                             cudaMemcpyHostToDevice, st));
-                        // the source frame must stay valid until the copy has run
-                        const int wrc = wait_stream(st, timeout_ms());
-                        release(clip, f);
+                        // the source frame must stay valid until the copy has
+                        // run: wait for the copy itself, not for earlier
+                        // requests' kernels on the stream. A wait that runs
+                        // out leaves the frame with the caller (not released:
+                        // the copy may still read it)
+                        VSF_CUDA(cudaEventRecord(ctx->direct_copy_done(), st));
+                        const int wrc = wait_event(ctx->direct_copy, timeout_ms());
                         if (wrc != VSFEEL_OK) return wrc;
+                        release(clip, f);
                         continue;
                     }
                     const int k = ctx->up_next;
@@ -1359,7 +1391,8 @@ int get_frame(vsfeel_bm3d* ctx, int n, bool with_ref,
     if (rc == VSFEEL_OK && *rs.status != 0) {
         rc = guarded(ctx, [&]() -> int {
             VSF_CUDA(cudaMemsetAsync(ctx->status.p, 0, sizeof(int), ctx->stream));
-            return fail(VSFEEL_E_CUDA, "internal error: a search window left the staged region");
+            ctx->invalidate_stacks();
+            return fail(VSFEEL_E_CUDA, status_text(*rs.status));
         });
     }
     if (rc == VSFEEL_OK) {

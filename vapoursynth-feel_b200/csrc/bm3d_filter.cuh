@@ -119,6 +119,59 @@ __device__ __forceinline__ float wiener_coefficients(float d[64], const float r[
     return __fdiv_rn(1.0f, sum);
 }
 
+// Aggregation (src/bm3d.comp:697-715). The reference adds (w*p + E) - E to
+// the numerator and (w + E) - E to the weight of every pixel of every
+// matched patch. The weight is one value per group, so a pixel's weight sum
+// is the sum of that value over the patches covering it: the filter adds it
+// once per patch, at the patch's origin, into the slice's weight-origin
+// plane, and the normaliser sums each pixel's 8x8 window of origins
+// (bm3d_kernels.cu). With the extractor (E = 2^e) every addend is a multiple
+// of ulp(E) and the sums are exact in any order, so the weights equal the
+// reference's bit for bit; without it they differ only in float rounding
+// order, as the reference's own atomics do from run to run.
+//
+// Numerators go to the slice's numerator plane with float atomics; `acc`,
+// when given, is a tile-owned shared-memory accumulator that takes the
+// patches of slice acc->z whose 8x8 footprint lies inside it (the caller
+// flushes it into the plane once, see TileAccumulator).
+struct TileAccumulator {
+    float* num;  // shared: pixel (fx0 + c, fy0 + r) at num[r*w + c], w x h pixels
+    float* org;  // shared: weight of origin (fx0 + c, fy0 + r) at org[r*(w-7) + c]
+    int z;       // slice held (-1: none)
+    int fx0, fy0, w, h;
+};
+
+__device__ __forceinline__ void scatter_group(const StackJob& job, const uint32_t mxy[8],
+                                              uint32_t zp, int sub, const float d[64], float w,
+                                              const TileAccumulator* acc = nullptr) {
+    const float E = job.extractor;
+    const float wv = __fsub_rn(__fadd_rn(w, E), E);
+    const int dpitch = job.dst_pitch;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const int z = (int)((zp >> (4 * k)) & 15u);
+        float* num = job.slice_dst[z];
+        if (num == nullptr) continue;
+        const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
+        if (acc && z == acc->z) {
+            const int c = mx - acc->fx0, r = my - acc->fy0;
+            if (c >= 0 && r >= 0 && c + 8 <= acc->w && r + 8 <= acc->h) {
+                float* pn = acc->num + r * acc->w + c + sub;
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    atomicAdd(pn + j * acc->w, __fsub_rn(__fmaf_rn(w, d[k * 8 + j], E), E));
+                if (sub == k) atomicAdd(acc->org + r * (acc->w - 7) + c, wv);
+                continue;
+            }
+        }
+        float* pn = num + (size_t)my * dpitch + mx + sub;
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+            atomicAdd(pn + (size_t)j * dpitch, __fsub_rn(__fmaf_rn(w, d[k * 8 + j], E), E));
+        if (sub == k) atomicAdd(num + job.dst_plane + (size_t)my * dpitch + mx, wv);
+    }
+}
+
 // Filters block b's group (matches mxy = x | y << 16, zp = 8 x 4-bit slice)
 // and scatters it into the stack's slices. kSaveMask also records the keep
 // bits, lane `sub` writing word mask_out[b * 8 + sub] (bit 8 * group
@@ -128,7 +181,7 @@ __device__ __forceinline__ float wiener_coefficients(float d[64], const float r[
 template <bool kSaveMask, bool kWiener = false>
 __device__ __forceinline__ void filter_group(const StackJob& job, int b, bool valid,
                                              const uint32_t mxy[8], uint32_t zp, int sub,
-                                             float* buf) {
+                                             float* buf, const TileAccumulator* acc = nullptr) {
     float d[64];
     float w;
     if (kWiener) {
@@ -161,23 +214,7 @@ __device__ __forceinline__ void filter_group(const StackJob& job, int b, bool va
     inverse3(d, buf, sub);
 
     if (!valid) return;
-    const float E = job.extractor;
-    const float wv = __fsub_rn(__fadd_rn(w, E), E);
-    const int dpitch = job.dst_pitch;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const int z = (int)((zp >> (4 * k)) & 15u);
-        float* num = job.slice_dst[z];
-        if (num == nullptr) continue;
-        const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
-        float* pn = num + (size_t)my * dpitch + mx + sub;
-        float* pd = pn + job.dst_plane;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            atomicAdd(pn + (size_t)j * dpitch, __fsub_rn(__fmaf_rn(w, d[k * 8 + j], E), E));
-            atomicAdd(pd + (size_t)j * dpitch, wv);
-        }
-    }
+    scatter_group(job, mxy, zp, sub, d, w, acc);
 }
 
 }  // namespace vsfeel

@@ -281,28 +281,67 @@ __global__ void __launch_bounds__(kGroups * 8) bm3d_filter_kernel(const StackJob
 }
 
 // ---------------------------------------------------------------------------
-// Four consecutive pixels (x0 .. x0+3) of one row: float4 loads from the
-// slices (their rows are padded to 32 floats, so the loads stay inside and
-// aligned), slice pointers indexed statically, each pixel's FP64 sums in
-// the reference's order i = 0..tw-1.
-__device__ __forceinline__ void normalize_px4(const NormalizeJob& job, int x0, int y) {
-    const size_t o = (size_t)y * job.src_pitch + x0;
+// Normalisation (src/bm3d_agg.comp:36-52): out = float(sum_i double(num_i) /
+// sum_i double(den_i)) over the tw slices, in the reference's order i = 0..tw-1.
+// A slice's weight plane holds per-patch weights at the patches' origins
+// (scatter_group): den_i of a pixel (x, y) is the sum of origins
+// x-7..x by y-7..y, taken in float as the 8 vertical sums of its columns,
+// then their sum from left to right.
+//
+// One warp covers 120 pixels of one row: lane l reads columns
+// x0 - 8 + 4l .. +3 of the 8 origin rows (one float4 each) and forms their
+// vertical sums; lanes 2..31 own the pixels x0 + 4(l-2) .. +3 and take the 7
+// vertical sums left of their own from lanes l-2 and l-1 by shuffles (lanes
+// 0 and 1 hold the tile's left halo). No shared memory, so the kernel's
+// CTAs fit beside the matcher's. Origin planes exist for 0..W-8 x 0..H-8
+// and are zero elsewhere within the padded plane; rows above the frame read
+// as zero. The numerator planes are read four floats at a time (rows
+// padded to 32 floats, bases 16-byte aligned).
+__device__ __forceinline__ void normalize_tile(const NormalizeJob& job, int tx0, int ty0) {
+    const int lane = threadIdx.x & 31;
+    const int y = ty0 + (threadIdx.x >> 5);
+    if (y >= job.height) return;  // whole warps leave: the shuffles below stay full
+    const int col = tx0 - 8 + 4 * lane;          // first origin column of this lane
+    const int x0 = tx0 + 4 * (lane - 2);         // first pixel of this lane (lanes >= 2)
+    const bool has_px = lane >= 2 && x0 < job.width;
+    const bool col_ok = col >= 0 && col + 3 < job.src_pitch;
     double acc[4] = {0.0, 0.0, 0.0, 0.0}, acw[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll 1
+    for (int i = 0; i < job.tw; ++i) {
+        const float* org = job.num[i] + job.den_offset;
+        float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-    for (int i = 0; i < kMaxTW; ++i) {
-        if (i < job.tw) {
-            const float4 a = *reinterpret_cast<const float4*>(job.num[i] + o);
-            const float4 w = *reinterpret_cast<const float4*>(job.num[i] + o + job.den_offset);
-            acc[0] += (double)a.x;
-            acc[1] += (double)a.y;
-            acc[2] += (double)a.z;
-            acc[3] += (double)a.w;
-            acw[0] += (double)w.x;
-            acw[1] += (double)w.y;
-            acw[2] += (double)w.z;
-            acw[3] += (double)w.w;
+        for (int dy = 7; dy >= 0; --dy) {
+            const int oy = y - dy;
+            float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (oy >= 0 && col_ok) a = *reinterpret_cast<const float4*>(org + (size_t)oy * job.src_pitch + col);
+            v[0] = __fadd_rn(v[0], a.x);
+            v[1] = __fadd_rn(v[1], a.y);
+            v[2] = __fadd_rn(v[2], a.z);
+            v[3] = __fadd_rn(v[3], a.w);
+        }
+        // vertical sums of columns c-8 .. c+3 (c = this lane's first column + 8)
+        float h[12];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            h[k] = __shfl_up_sync(0xffffffffu, v[k], 2);
+            h[4 + k] = __shfl_up_sync(0xffffffffu, v[k], 1);
+            h[8 + k] = v[k];
+        }
+        float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (has_px) a = *reinterpret_cast<const float4*>(job.num[i] + (size_t)y * job.src_pitch + x0);
+        const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            // pixel x0 + k: origins x0+k-7 .. x0+k, h[k+1] .. h[k+8]
+            float w = h[k + 1];
+#pragma unroll
+            for (int dx = 2; dx <= 8; ++dx) w = __fadd_rn(w, h[k + dx]);
+            acc[k] += (double)av[k];
+            acw[k] += (double)w;
         }
     }
+    if (!has_px) return;
     float* out = job.out + (size_t)y * job.out_pitch;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -313,12 +352,8 @@ __device__ __forceinline__ void normalize_px4(const NormalizeJob& job, int x0, i
     }
 }
 
-// One CTA: 128 x 8 pixels, 4 per thread.
 __global__ void __launch_bounds__(256) bm3d_normalize_kernel(const NormalizeJob job) {
-    const int x0 = (blockIdx.x * 32 + (threadIdx.x & 31)) * 4;
-    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
-    if (x0 >= job.width || y >= job.height) return;
-    normalize_px4(job, x0, y);
+    normalize_tile(job, blockIdx.x * kNormTileW, blockIdx.y * kNormTileH);
 }
 
 // Batched form: the filter of 16 blocks of one stack per CTA.
@@ -359,11 +394,8 @@ __global__ void __launch_bounds__(256) bm3d_normalize_batch_kernel(const Normali
     }
     const NormalizeJob& job = work.jobs[lo];
     const int t = item - work.tile_first[lo];
-    const int tiles_x = (job.width + 127) / 128;
-    const int x0 = ((t % tiles_x) * 32 + (threadIdx.x & 31)) * 4;
-    const int y = (t / tiles_x) * 8 + (threadIdx.x >> 5);
-    if (x0 >= job.width || y >= job.height) return;
-    normalize_px4(job, x0, y);
+    const int tiles_x = (job.width + kNormTileW - 1) / kNormTileW;
+    normalize_tile(job, (t % tiles_x) * kNormTileW, (t / tiles_x) * kNormTileH);
 }
 
 // ---------------------------------------------------------------------------
@@ -519,7 +551,7 @@ cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream) {
 }
 
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream) {
-    dim3 grid((job.width + 127) / 128, (job.height + 7) / 8);
+    dim3 grid((job.width + kNormTileW - 1) / kNormTileW, (job.height + kNormTileH - 1) / kNormTileH);
     bm3d_normalize_kernel<<<grid, 256, 0, stream>>>(job);
     return cudaGetLastError();
 }

@@ -10,8 +10,8 @@ namespace vsfeel {
 #define VSFEEL_TILE_DECL(TX, TY)                                                              \
     size_t tile_plan_bytes_##TX##x##TY(const StackJob& job, TileMode mode);                   \
     cudaError_t launch_tiles_##TX##x##TY(const StackJob& job, TileMode mode, cudaStream_t s); \
-    cudaError_t launch_batch_##TX##x##TY(const BatchWork& work, TileMode mode, size_t smem,   \
-                                         int grid, cudaStream_t s);
+    cudaError_t launch_batch_##TX##x##TY(const BatchWork& work, TileMode mode, int lanes,     \
+                                         size_t smem, int grid, cudaStream_t s);
 VSFEEL_TILE_DECL(8, 4)
 VSFEEL_TILE_DECL(16, 2)
 VSFEEL_TILE_DECL(4, 8)
@@ -96,14 +96,15 @@ cudaError_t launch_match_tiles(const StackJob& job, TileShape shape, TileMode mo
     }
 }
 
-cudaError_t launch_batch_tiles(const BatchWork& work, TileShape shape, TileMode mode, size_t smem,
-                               int grid, cudaStream_t stream) {
+cudaError_t launch_batch_tiles(const BatchWork& work, TileShape shape, TileMode mode, int lanes,
+                               size_t smem, int grid, cudaStream_t stream) {
+    if (lanes != 8 && (lanes != 16 || mode != kTableOnly)) return cudaErrorInvalidValue;
     switch (shape) {
-        case kTile8x4: return launch_batch_8x4(work, mode, smem, grid, stream);
-        case kTile16x2: return launch_batch_16x2(work, mode, smem, grid, stream);
-        case kTile4x8: return launch_batch_4x8(work, mode, smem, grid, stream);
-        case kTile8x2: return launch_batch_8x2(work, mode, smem, grid, stream);
-        default: return launch_batch_4x4(work, mode, smem, grid, stream);
+        case kTile8x4: return launch_batch_8x4(work, mode, lanes, smem, grid, stream);
+        case kTile16x2: return launch_batch_16x2(work, mode, lanes, smem, grid, stream);
+        case kTile4x8: return launch_batch_4x8(work, mode, lanes, smem, grid, stream);
+        case kTile8x2: return launch_batch_8x2(work, mode, lanes, smem, grid, stream);
+        default: return launch_batch_4x4(work, mode, lanes, smem, grid, stream);
     }
 }
 

@@ -60,6 +60,7 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kMinK = 2, kMaxK = 5;
 constexpr int kCollect = 64;                // candidates a block collects per pass
 constexpr int kLaneChunks = 4;              // chunks with hits a lane notes (first pass)
+constexpr int kMaxSelectPasses = 64;        // bound tightenings before a table is deemed corrupt
 constexpr uint64_t kKeyMax = (uint64_t(0x7f7fffffu) << 32) | 0x7fffffffu;  // (FLT_MAX, INT_MAX)
 
 __device__ __forceinline__ uint64_t make_key(float err, int seq) {
@@ -410,8 +411,13 @@ __device__ __forceinline__ void scan_chunk_exact(const Region& reg, const float*
     }
 }
 
+// Rows per lane of the sliding scan: the lanes of a block share its window
+// rows; 16 lanes per block carry at most 3 rows each (the 512-thread form
+// runs at 128 registers per thread).
+template <int kLanes>
 __device__ __forceinline__ int rows_per_lane(int total_rows) {
-    return min(kMaxK, max(kMinK, (total_rows + 7) / 8));
+    constexpr int kMax = kLanes == 8 ? kMaxK : 3;
+    return min(kMax, max(kMinK, (total_rows + kLanes - 1) / kLanes));
 }
 
 // A block's global match list, spatial predictors, the phase's top-8 and the
@@ -457,15 +463,16 @@ __device__ __forceinline__ void merge_top8(uint64_t top[8], GroupState* gs, unsi
 // gs->top (padded with (FLT_MAX, INT_MAX) when fewer exist; errors >= FLT_MAX
 // never count, as in the reference). lb: this lane's 8 smallest per-row
 // minima (ascending). All 8 lanes of the group take part.
+template <int kLanes>
 __device__ void select_top8(const float* E, const Window* wins, int nwin, float lb[8],
-                            GroupState* gs, unsigned gmask) {
-    const int sub = threadIdx.x & 7;
+                            GroupState* gs, unsigned gmask, int* status) {
+    const int sub = threadIdx.x & (kLanes - 1);
     // bound: the 8th smallest of the rows' three smallest errors -- at least 8
     // candidates lie at or below it. Each lane's list is sorted; three
     // bitonic merge stages with the lanes 1, 2 and 4 apart leave every lane
     // with the group's 8 smallest, sorted.
 #pragma unroll
-    for (int off = 1; off < 8; off <<= 1) {
+    for (int off = 1; off < kLanes; off <<= 1) {
         float o[8];
 #pragma unroll
         for (int i = 0; i < 8; ++i) o[i] = __shfl_xor_sync(gmask, lb[i], off);
@@ -505,11 +512,11 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
             const int n_w = w.rw * w.h;
             const int nq = (n_w + 3) >> 2;
             const float4* tab = reinterpret_cast<const float4*>(E + w.eoff);
-            for (int v0 = 0; v0 < nq; v0 += 32) {
+            for (int v0 = 0; v0 < nq; v0 += 4 * kLanes) {
                 float4 q[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    const int v = v0 + sub + 8 * k;
+                    const int v = v0 + sub + kLanes * k;
                     q[k] = v < nq ? tab[v] : make_float4(kFltMax, kFltMax, kFltMax, kFltMax);
                 }
                 float mn = kFltMax;
@@ -523,7 +530,7 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
                     const float ev[4] = {q[k].x, q[k].y, q[k].z, q[k].w};
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
-                        const int f = 4 * (v0 + sub + 8 * k) + u;
+                        const int f = 4 * (v0 + sub + kLanes * k) + u;
                         const bool hit = f < n_w && ev[u] <= terr && ev[u] < kFltMax;
                         mask |= hit ? (1u << (4 * k + u)) : 0u;
                     }
@@ -543,11 +550,11 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
         for (int i = 0; i < kLaneChunks; ++i) cnt += __popc(cm[i]);
         int incl = cnt;
 #pragma unroll
-        for (int off = 1; off < 8; off <<= 1) {
-            const int t = __shfl_up_sync(gmask, incl, off, 8);
+        for (int off = 1; off < kLanes; off <<= 1) {
+            const int t = __shfl_up_sync(gmask, incl, off, kLanes);
             if (sub >= off) incl += t;
         }
-        const int total = __shfl_sync(gmask, incl, 7, 8);
+        const int total = __shfl_sync(gmask, incl, kLanes - 1, kLanes);
         const bool overflow = __any_sync(gmask, nc > kLaneChunks) || total > kCollect;
         if (!overflow) {
             int pos = incl - cnt;
@@ -559,7 +566,7 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
                 while (m) {
                     const int b = __ffs(m) - 1;
                     m &= m - 1;
-                    const int f = 4 * (v0 + sub + 8 * (b >> 2)) + (b & 3);
+                    const int f = 4 * (v0 + sub + kLanes * (b >> 2)) + (b & 3);
                     const int d = div_small(f, w.h);
                     const int row = f - d * w.h;
                     gs->buf[pos++] = make_key(E[w.eoff + f], w.seq_base + row * w.rw + d);
@@ -570,7 +577,15 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
         }
         __syncwarp(gmask);
     }
-    while (!fast) {
+    // every pass at least shrinks the set of keys at or below the bound
+    // (errors are sums of squares, never negative); the cap only guards
+    // against a corrupted table, and reports it
+    for (int pass = 0; !fast; ++pass) {
+        if (pass == kMaxSelectPasses) {
+            if (sub == 0) atomicOr(status, 2);
+            n = kCollect;
+            break;
+        }
         if (sub == 0) gs->count = 0;
         __syncwarp(gmask);
         const float terr = key_err(tkey);
@@ -585,11 +600,11 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
             const int n_w = w.rw * w.h;
             const int nq = (n_w + 3) >> 2;
             const float4* tab = reinterpret_cast<const float4*>(E + w.eoff);
-            for (int v0 = 0; v0 < nq; v0 += 32) {
+            for (int v0 = 0; v0 < nq; v0 += 4 * kLanes) {
                 float4 q[4];
 #pragma unroll
                 for (int k = 0; k < 4; ++k) {
-                    const int v = v0 + sub + 8 * k;
+                    const int v = v0 + sub + kLanes * k;
                     q[k] = v < nq ? tab[v] : make_float4(kFltMax, kFltMax, kFltMax, kFltMax);
                 }
                 float mn = kFltMax;
@@ -602,7 +617,7 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
                     const float ev[4] = {q[k].x, q[k].y, q[k].z, q[k].w};
 #pragma unroll
                     for (int u = 0; u < 4; ++u) {
-                        const int f = 4 * (v0 + sub + 8 * k) + u;
+                        const int f = 4 * (v0 + sub + kLanes * k) + u;
                         if (f < n_w && ev[u] <= terr && ev[u] < kFltMax) {
                             const int d = div_small(f, w.h);
                             const int row = f - d * w.h;
@@ -622,23 +637,23 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
         // more than kCollect at or below the bound: tighten it to the 8th
         // smallest key among the collected ones and collect again
         uint64_t t8 = kKeyMax;
-        for (int j = sub; j < kCollect; j += 8) {
+        for (int j = sub; j < kCollect; j += kLanes) {
             const uint64_t kj = gs->buf[j];
             int rank = 0;
             for (int i = 0; i < kCollect; ++i) rank += gs->buf[i] < kj ? 1 : 0;
             if (rank == 7) t8 = kj;
         }
 #pragma unroll
-        for (int off = 1; off < 8; off <<= 1) {
+        for (int off = 1; off < kLanes; off <<= 1) {
             const uint64_t o = __shfl_xor_sync(gmask, t8, off);
             t8 = o < t8 ? o : t8;
         }
         tkey = t8;
         __syncwarp(gmask);
     }
-    gs->top[sub] = kKeyMax;
+    if (sub < 8) gs->top[sub] = kKeyMax;
     __syncwarp(gmask);
-    for (int j = sub; j < n; j += 8) {
+    for (int j = sub; j < n; j += kLanes) {
         const uint64_t kj = gs->buf[j];
         int rank = 0;
         for (int i = 0; i < n; ++i) rank += gs->buf[i] < kj ? 1 : 0;
@@ -650,11 +665,12 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
 // Scans windows[0..nwin) of this lane's block into its error table, then
 // selects the top-8 into gs->top. Rows are split into chunks of K
 // (warp-uniform); chunk c of the block goes to lane c % 8 in round c / 8.
-template <bool kExact>
+template <bool kExact, int kLanes>
 __device__ void search_windows(const Region& reg, const float* cur_s, const float c7[8],
                                const Window* wins, int nwin, float* E, GroupState* gs,
-                               unsigned gmask, int* status) {
-    const int sub = threadIdx.x & 7;
+                               unsigned gmask, int* status, bool probe) {
+    static_assert(kLanes == 8 || (kLanes == 16 && !kExact), "16 lanes: sliding scan only");
+    const int sub = threadIdx.x & (kLanes - 1);
     int total_rows = 0;
     for (int i = 0; i < nwin; ++i) total_rows += wins[i].h;
     // the exact scan keeps 8 column sums per row: 2 or 3 rows per lane,
@@ -673,11 +689,11 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
         const int c3 = (t3 + 7) / 8 * kStep3;
         K = warp_max(c3 < c2 ? 3 : 2);
     } else {
-        K = warp_max(rows_per_lane(total_rows));
+        K = warp_max(rows_per_lane<kLanes>(total_rows));
     }
     int ntasks = 0;
     for (int i = 0; i < nwin; ++i) ntasks += qdiv<kExact>(wins[i].h + K - 1, K);
-    const int rounds = warp_max((ntasks + 7) / 8);
+    const int rounds = warp_max((ntasks + kLanes - 1) / kLanes);
     float lb[8];
     uint64_t top[8];
 #pragma unroll
@@ -685,8 +701,9 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
         lb[i] = kFltMax;
         top[i] = kKeyMax;
     }
+    bool skipped = false;  // a window of this lane left the staged region (not scanned)
     for (int round = 0; round < rounds; ++round) {
-        const int task = round * 8 + sub;
+        const int task = round * kLanes + sub;
         const bool has = task < ntasks;
         int wi = 0, c = has ? task : 0;
         while (wi < nwin - 1 && c >= qdiv<kExact>(wins[wi].h + K - 1, K)) {
@@ -699,9 +716,11 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
         // every window lies inside the staged region by construction (the
         // host routes configurations that could place one outside to the
         // direct-read kernel); should one not, scan nothing here and report
-        if (win.left < reg.rx0 || win.left + win.rw + 6 > reg.rx1 || win.top < reg.ry0 ||
+        // (`probe`: the host's test hook makes this tile report)
+        if (probe || win.left < reg.rx0 || win.left + win.rw + 6 > reg.rx1 || win.top < reg.ry0 ||
             win.top + win.h + 6 > reg.ry1) {
             if (has) atomicOr(status, 1);
+            skipped = skipped || has;
             win = Window{reg.rx0, reg.ry0, 1, 1, 0, 0};
             r0 = reg.ry0;
             nrows = 0;
@@ -713,6 +732,11 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
                 case 2: scan_chunk_exact<2>(reg, E, win, r0, nrows, jcount, top); break;
                 default: scan_chunk_exact<3>(reg, E, win, r0, nrows, jcount, top); break;
             }
+        } else if (kLanes == 16) {
+            if (K == 2)
+                scan_chunk<2>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb);
+            else
+                scan_chunk<3>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb);
         } else {
             switch (K) {
                 case 2: scan_chunk<2>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb); break;
@@ -723,10 +747,17 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
         }
     }
     __syncwarp(gmask);
-    if (kExact)
+    // a group with an unscanned window has no valid errors to select from
+    // (its table holds stale values): it reports sentinels only
+    if (__any_sync(gmask, skipped)) {
+        if (sub < 8) gs->top[sub] = kKeyMax;
+        __syncwarp(gmask);
+        return;
+    }
+    if constexpr (kExact)
         merge_top8(top, gs, gmask);
     else
-        select_top8(E, wins, nwin, lb, gs, gmask);
+        select_top8<kLanes>(E, wins, nwin, lb, gs, gmask, status);
 }
 
 // Position of a key. Sentinels decode to (0, 0) as in the reference.
@@ -788,17 +819,39 @@ __host__ __device__ inline int window_slots(const StackJob& job) {
 }
 
 struct SmemPlan {
-    int region_floats;  // staged region
-    int estride;        // floats per block error table (== 8 mod 32)
-    int etab_floats;    // all error tables (also the fused filter's buffers)
+    int region_floats;     // staged region
+    int estride;           // floats per block error table (== 8 mod 32)
+    int etab_floats;       // all error tables (also the fused filter's buffers), a multiple of 4
+    size_t region_offset;  // bytes from the dynamic shared memory's base to the region
     size_t bytes;
 };
+
+// The layout match_tile carves (block state, windows, reference blocks,
+// tables, region) keeps the tables' float4 reads and the region's 8-byte
+// reads aligned; launchers check it before every launch.
+template <int TX, int TY>
+__host__ inline bool smem_plan_aligned(const SmemPlan& p) {
+    const size_t cur = p.region_offset - sizeof(float) * (size_t(TX * TY) * 64 + p.etab_floats);
+    return cur % 16 == 0 && p.region_offset % 16 == 0;
+}
 
 __host__ __device__ inline int error_table_floats(const StackJob& job) {
     const int ws = 2 * job.bm_range + 1, wt = 2 * job.ps_range + 1;
     const int spatial = (ws * ws + 3) & ~3;
     const int temporal = job.radius > 0 ? job.ps_num * ((wt * wt + 3) & ~3) : 0;
     return spatial > temporal ? spatial : temporal;
+}
+
+// The fused modes' tile accumulator for slice r: every spatial match of the
+// tile's blocks lies within bm_range of a block, so its patches cover at most
+// (tile + 2 bm_range) pixels per axis (numerators), and their origins that
+// less 7 (weights).
+template <int TX, int TY>
+__host__ __device__ inline int accumulator_floats(const StackJob& job) {
+    const int tw = (TX - 1) * job.step + 8 + 2 * job.bm_range;
+    const int th = (TY - 1) * job.step + 8 + 2 * job.bm_range;
+    const int w = tw < job.width ? tw : job.width, h = th < job.height ? th : job.height;
+    return w * h + (w - 7) * (h - 7);
 }
 
 template <int TX, int TY>
@@ -818,10 +871,15 @@ __host__ __device__ inline SmemPlan smem_plan(const StackJob& job, int mode) {
     const int tf = error_table_floats(job);
     p.estride = job.radius >= 3 ? 64 : tf + ((8 - tf) & 31);  // the least >= tf that is 8 mod 32
     p.etab_floats = kGroups * p.estride;
-    if (mode != kTableOnly && p.etab_floats < kGroups * kGroupStride)
-        p.etab_floats = kGroups * kGroupStride;
-    p.bytes = sizeof(float) * (size_t(kGroups) * 64 + size_t(p.etab_floats) + p.region_floats) +
-              sizeof(Window) * kGroups * window_slots(job) + sizeof(GroupState) * kGroups;
+    // fused modes: the filter's transposes, then the slice-r accumulator
+    const int fused_floats = kGroups * kGroupStride + accumulator_floats<TX, TY>(job);
+    if (mode != kTableOnly && p.etab_floats < fused_floats) p.etab_floats = fused_floats;
+    // the staged region follows the tables and is read as 8-byte pairs: keep
+    // it on a 16-byte boundary
+    p.etab_floats = (p.etab_floats + 3) & ~3;
+    p.region_offset = sizeof(GroupState) * kGroups + sizeof(Window) * kGroups * window_slots(job) +
+                      sizeof(float) * (size_t(kGroups) * 64 + size_t(p.etab_floats));
+    p.bytes = p.region_offset + sizeof(float) * p.region_floats;
     return p;
 }
 
@@ -829,9 +887,11 @@ __host__ __device__ inline SmemPlan smem_plan(const StackJob& job, int mode) {
 // filtering of their groups. Shared memory: block state, windows, reference
 // blocks, error tables (the fused filter's buffers afterwards), then the
 // staged region. Every thread of the CTA calls it.
-template <int TX, int TY, int kMode, bool kExact = false>
+template <int TX, int TY, int kMode, bool kExact = false, int kLanes = 8>
 __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
                                            unsigned char* smem_raw) {
+    static_assert(kLanes == 8 || (kLanes == 16 && kMode == kTableOnly && !kExact),
+                  "16 lanes per block: the sliding scan writing match tables");
     constexpr int kGroups = TX * TY;
     const SmemPlan plan = smem_plan<TX, TY>(job, kMode);
     GroupState* gs_all = reinterpret_cast<GroupState*>(smem_raw);
@@ -840,18 +900,24 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
     float* etab_all = cur_all + kGroups * 64;
     float* region = etab_all + (size_t)plan.etab_floats;
 
+    // kLanes lanes per block (group); a warp holds kGpw groups. Lane `sub`
+    // of a group holds entry sub & 7 of the block's match list (lanes 8..15
+    // of a 16-lane group mirror lanes 0..7: every list operation runs in
+    // 8-lane segments)
+    constexpr int kGpw = 32 / kLanes;
     const int lane = threadIdx.x & 31;
-    const int sub = lane & 7;
-    const int g = threadIdx.x >> 3;         // group in the CTA
-    const int wrp = g >> 2, gi = g & 3;     // warp, group in the warp
-    const unsigned gmask = 0xffu << (lane & ~7);
+    const int sub = lane & (kLanes - 1);
+    const int ent = sub & 7;
+    const int g = threadIdx.x / kLanes;     // group in the CTA
+    const int wrp = g / kGpw, gi = g % kGpw;  // warp, group in the warp
+    const unsigned gmask = (kLanes == 8 ? 0xffu : 0xffffu) << (lane & ~(kLanes - 1));
     const int tiles_x = (job.nbx + TX - 1) / TX;
     const int tx = tile % tiles_x, ty = tile / tiles_x;
     const int bx0 = tx * TX, by0 = ty * TY;
     const int bx_last = min(bx0 + TX - 1, job.nbx - 1);
     const int by_last = min(by0 + TY - 1, job.nby - 1);
-    // warp wrp: block row wrp / (TX/4), block columns o + (TX/4) * {0, 1, 2, 3}
-    constexpr int kWarpsPerRow = TX / 4;
+    // warp wrp: block row wrp / (TX/kGpw), block columns o + (TX/kGpw) * gi
+    constexpr int kWarpsPerRow = TX / kGpw;
     const int bxr = bx0 + (wrp % kWarpsPerRow) + kWarpsPerRow * gi;
     const int byr = by0 + wrp / kWarpsPerRow;
     const bool valid = bxr < job.nbx && byr < job.nby;
@@ -864,14 +930,17 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
     const int r = job.radius;
     const int R = job.bm_range, Q = job.ps_range, P = job.ps_num;
     const int pitch = job.pitch;
+    const bool probe = job.probe_tile == tile + 1;
 
     float* cur_s = cur_all + g * 64;
     float* E = etab_all + (size_t)g * plan.estride;
     Window* win = win_all + g * window_slots(job);
     GroupState* gs = gs_all + g;
     const float* fc = job.slice_frame[r];
+    if (sub < 8) {
 #pragma unroll
-    for (int i = 0; i < 8; ++i) cur_s[sub * 8 + i] = __ldg(fc + (size_t)(y + i) * pitch + x + sub);
+        for (int i = 0; i < 8; ++i) cur_s[sub * 8 + i] = __ldg(fc + (size_t)(y + i) * pitch + x + sub);
+    }
     __syncwarp(gmask);
     float c7[8];
 #pragma unroll
@@ -917,21 +986,21 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         const Region s = stage(fc, R);
         if (sub == 0) win[0] = make_window(x, y, R, W, H, 0, 0);
         __syncwarp(gmask);
-        search_windows<kExact>(s, cur_s, c7, win, 1, E, gs, gmask, job.status);
-        const uint64_t k = gs->top[sub];
+        search_windows<kExact, kLanes>(s, cur_s, c7, win, 1, E, gs, gmask, job.status, probe);
+        const uint64_t k = gs->top[ent];
         const uint32_t xy = key_xy<kExact>(k, win, 0);
-        // the global match list: lane `sub` holds entry sub
+        // the global match list: lane `sub` holds entry sub & 7
         ge = key_err(k);
         gxy = xy;
         gz = r;
-        gs->sxy[sub] = xy;
+        if (sub < 8) gs->sxy[sub] = xy;
         __syncwarp(gmask);
     }
 
     // temporal predictive search (src/bm3d.comp:540-637)
     const int area = (2 * Q + 1) * (2 * Q + 1);
     for (int dir = -1; dir <= 1; dir += 2) {
-        gs->pxy[sub] = gs->sxy[sub];
+        if (sub < 8) gs->pxy[sub] = gs->sxy[sub];
         __syncwarp(gmask);
         for (int t = 1; t <= r; ++t) {
             const int z = r + dir * t;
@@ -945,7 +1014,7 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
                 }
             }
             __syncwarp(gmask);
-            search_windows<kExact>(s, cur_s, c7, win, P, E, gs, gmask, job.status);
+            search_windows<kExact, kLanes>(s, cur_s, c7, win, P, E, gs, gmask, job.status, probe);
             // the frame's first P matches enter the global list in order with
             // the reference's strict < (src/bm3d.comp:304-322): an entry goes
             // after the ones it does not beat; the group's lanes shift in
@@ -961,11 +1030,11 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
                 const int pz = __shfl_up_sync(gmask, gz, 1, 8);
                 if (err < e7) {
                     const int pos = __popc((below >> (lane & ~7)) & 0xffu);
-                    if (sub > pos) {
+                    if (ent > pos) {
                         ge = pe;
                         gxy = pxy;
                         gz = pz;
-                    } else if (sub == pos) {
+                    } else if (ent == pos) {
                         ge = err;
                         gxy = fxy;
                         gz = z;
@@ -985,13 +1054,13 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         const uint32_t pxy = __shfl_up_sync(gmask, gxy, 1, 8);
         const int pz = __shfl_up_sync(gmask, gz, 1, 8);
         if (!has_self) {
-            gxy = sub == 0 ? self_xy : pxy;
-            gz = sub == 0 ? r : pz;
+            gxy = ent == 0 ? self_xy : pxy;
+            gz = ent == 0 ? r : pz;
         }
-        const uint32_t zp = __reduce_or_sync(gmask, uint32_t(gz) << (4 * sub));
-        gs->gxy[sub] = gxy;
+        const uint32_t zp = __reduce_or_sync(gmask, sub < 8 ? uint32_t(gz) << (4 * sub) : 0u);
+        if (sub < 8) gs->gxy[sub] = gxy;
         if (sub == 0) gs->gz[0] = int(zp);
-        if (valid && kMode != kFused) {
+        if (valid && kMode != kFused && sub < 8) {
             const size_t b = (size_t)by * job.nbx + bx;
             job.match_xy[b * 8 + sub] = gxy;
             if (sub == 0) job.match_z[b] = zp;
@@ -1004,19 +1073,51 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
 #pragma unroll
         for (int k = 0; k < 8; ++k) mxy[k] = gs->gxy[k];
         const uint32_t zp = uint32_t(gs->gz[0]);
-        // the filter's transposes reuse the error tables: every group of the
-        // CTA must be done selecting
+        // the filter's transposes and the tile's accumulator for slice r
+        // (TileAccumulator) reuse the error tables: every group of the CTA
+        // must be done selecting
+        TileAccumulator acc;
+        acc.z = job.slice_dst[r] ? r : -1;
+        acc.fx0 = max(tile_x0 - R, 0);
+        acc.fy0 = max(tile_y0 - R, 0);
+        acc.w = min(tile_x1 + R, W - 8) + 8 - acc.fx0;
+        acc.h = min(tile_y1 + R, H - 8) + 8 - acc.fy0;
+        acc.num = etab_all + (size_t)kGroups * kGroupStride;
+        acc.org = acc.num + acc.w * acc.h;
+        const int nacc = acc.w * acc.h + (acc.w - 7) * (acc.h - 7);
+        __syncthreads();
+        if (acc.z >= 0)
+            for (int e = threadIdx.x; e < nacc; e += blockDim.x) acc.num[e] = 0.0f;
         __syncthreads();
         const int b = by * job.nbx + bx;
         filter_group<kMode == kFusedSave>(job, b, valid, mxy, zp, sub,
-                                           etab_all + (size_t)g * kGroupStride);
+                                           etab_all + (size_t)g * kGroupStride, &acc);
+        __syncthreads();
+        // flush: one atomic per covered pixel and per weighted origin (zero
+        // sums are skipped; adding +0.0 changes nothing)
+        if (acc.z >= 0) {
+            float* num = job.slice_dst[r];
+            const int dp = job.dst_pitch;
+            for (int e = threadIdx.x; e < acc.w * acc.h; e += blockDim.x) {
+                const float v = acc.num[e];
+                const int rr = e / acc.w, cc = e - rr * acc.w;
+                if (v != 0.0f) atomicAdd(num + (size_t)(acc.fy0 + rr) * dp + acc.fx0 + cc, v);
+            }
+            const int ow = acc.w - 7;
+            for (int e = threadIdx.x; e < ow * (acc.h - 7); e += blockDim.x) {
+                const float v = acc.org[e];
+                const int rr = e / ow, cc = e - rr * ow;
+                if (v != 0.0f)
+                    atomicAdd(num + job.dst_plane + (size_t)(acc.fy0 + rr) * dp + acc.fx0 + cc, v);
+            }
+        }
     }
 }
 
-template <int TX, int TY, int kMode>
-__global__ void __launch_bounds__(TX * TY * 8, 1) bm3d_match_sliding_kernel(const StackJob job) {
+template <int TX, int TY, int kMode, int kLanes = 8>
+__global__ void __launch_bounds__(TX * TY * kLanes, 1) bm3d_match_sliding_kernel(const StackJob job) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    match_tile<TX, TY, kMode>(job, blockIdx.x, smem_raw);
+    match_tile<TX, TY, kMode, false, kLanes>(job, blockIdx.x, smem_raw);
 }
 
 // radius >= 3: the same tile body with the exact scan (match table only)
@@ -1030,8 +1131,8 @@ __global__ void __launch_bounds__(TX * TY * 8, 1) bm3d_match_exact_kernel(const 
 // Thread 0 claims the next item while the current one runs (the atomic's
 // latency hides behind the tile), and the item's StackJob is copied to
 // shared memory only when the item belongs to another stack than the last.
-template <int TX, int TY, int kMode>
-__global__ void __launch_bounds__(TX * TY * 8, 1) bm3d_batch_tile_kernel(const BatchWork work) {
+template <int TX, int TY, int kMode, int kLanes = 8>
+__global__ void __launch_bounds__(TX * TY * kLanes, 1) bm3d_batch_tile_kernel(const BatchWork work) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ StackJob s_job;
     __shared__ int s_item, s_job_index, s_first, s_end;
@@ -1069,7 +1170,7 @@ __global__ void __launch_bounds__(TX * TY * 8, 1) bm3d_batch_tile_kernel(const B
         }
         int next = 0;
         if (threadIdx.x == 0) next = atomicAdd(work.counter, 1);
-        match_tile<TX, TY, kMode>(s_job, item - s_first, smem_raw);
+        match_tile<TX, TY, kMode, false, kLanes>(s_job, item - s_first, smem_raw);
         __syncthreads();  // every thread has read s_item and s_first
         if (threadIdx.x == 0) s_item = next;
     }
@@ -1078,19 +1179,21 @@ __global__ void __launch_bounds__(TX * TY * 8, 1) bm3d_batch_tile_kernel(const B
 // ---------------------------------------------------------------------------
 // Launch templates, instantiated once per tile shape (bm3d_match_<shape>.cu).
 
-template <int TX, int TY, int kMode>
+template <int TX, int TY, int kMode, int kLanes = 8>
 cudaError_t launch_grid(const StackJob& job, size_t smem, cudaStream_t stream) {
-    auto* fn = bm3d_match_sliding_kernel<TX, TY, kMode>;
+    auto* fn = bm3d_match_sliding_kernel<TX, TY, kMode, kLanes>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int tiles = ((job.nbx + TX - 1) / TX) * ((job.nby + TY - 1) / TY);
-    fn<<<tiles, TX * TY * 8, smem, stream>>>(job);
+    fn<<<tiles, TX * TY * kLanes, smem, stream>>>(job);
     return cudaGetLastError();
 }
 
 template <int TX, int TY>
 cudaError_t launch_grid_mode(const StackJob& job, TileMode mode, cudaStream_t stream) {
-    const size_t smem = smem_plan<TX, TY>(job, mode).bytes;
+    const SmemPlan plan = smem_plan<TX, TY>(job, mode);
+    if (!smem_plan_aligned<TX, TY>(plan)) return cudaErrorMisalignedAddress;
+    const size_t smem = plan.bytes;
     if (job.radius >= 3) {
         if (mode != kTableOnly) return cudaErrorInvalidValue;
         auto* fn = bm3d_match_exact_kernel<TX, TY>;
@@ -1102,20 +1205,26 @@ cudaError_t launch_grid_mode(const StackJob& job, TileMode mode, cudaStream_t st
         return cudaGetLastError();
     }
     switch (mode) {
-        case kTableOnly: return launch_grid<TX, TY, kTableOnly>(job, smem, stream);
+        case kTableOnly:
+            return job.lanes == 16 ? launch_grid<TX, TY, kTableOnly, 16>(job, smem, stream)
+                                   : launch_grid<TX, TY, kTableOnly>(job, smem, stream);
         case kFused: return launch_grid<TX, TY, kFused>(job, smem, stream);
         default: return launch_grid<TX, TY, kFusedSave>(job, smem, stream);
     }
 }
 
 template <int TX, int TY>
-cudaError_t launch_batch(const BatchWork& work, TileMode mode, size_t smem, int grid,
+cudaError_t launch_batch(const BatchWork& work, TileMode mode, int lanes, size_t smem, int grid,
                          cudaStream_t stream) {
+    // (the batch's jobs were checked one by one when it was built:
+    // tile_smem_bytes refuses a misaligned plan)
     auto* fn = mode == kFused ? bm3d_batch_tile_kernel<TX, TY, kFused>
-                              : bm3d_batch_tile_kernel<TX, TY, kTableOnly>;
+                              : (lanes == 16 ? bm3d_batch_tile_kernel<TX, TY, kTableOnly, 16>
+                                             : bm3d_batch_tile_kernel<TX, TY, kTableOnly>);
+    if (mode == kFused && lanes != 8) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    fn<<<grid, TX * TY * 8, smem, stream>>>(work);
+    fn<<<grid, TX * TY * lanes, smem, stream>>>(work);
     return cudaGetLastError();
 }
 

@@ -1,19 +1,23 @@
 // Tiled matcher instantiated for 4x8-block tiles (kernels in bm3d_match.cuh).
 #include "bm3d_match.cuh"
 
+#include <cstdint>
+
 namespace vsfeel {
 
 size_t tile_plan_bytes_4x8(const StackJob& job, TileMode mode) {
-    return smem_plan<4, 8>(job, mode).bytes;
+    // an unaligned layout never fits (launch_grid_mode refuses it too)
+    const SmemPlan p = smem_plan<4, 8>(job, mode);
+    return smem_plan_aligned<4, 8>(p) ? p.bytes : SIZE_MAX;
 }
 
 cudaError_t launch_tiles_4x8(const StackJob& job, TileMode mode, cudaStream_t s) {
     return launch_grid_mode<4, 8>(job, mode, s);
 }
 
-cudaError_t launch_batch_4x8(const BatchWork& work, TileMode mode, size_t smem, int grid,
-                                 cudaStream_t s) {
-    return launch_batch<4, 8>(work, mode, smem, grid, s);
+cudaError_t launch_batch_4x8(const BatchWork& work, TileMode mode, int lanes, size_t smem,
+                                 int grid, cudaStream_t s) {
+    return launch_batch<4, 8>(work, mode, lanes, smem, grid, s);
 }
 
 }  // namespace vsfeel

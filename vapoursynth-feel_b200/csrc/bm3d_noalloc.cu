@@ -13,9 +13,14 @@
 // array until the process exits.
 //
 // The array's name is a host-side stand-in in host code, not a device
-// address: on each device, the first call resolves the real address with
-// cudaGetSymbolAddress while that device is current and caches it. That
-// first call per device should therefore come before any stream capture.
+// address. The real address belongs to a CUDA context: the first call in
+// each context resolves it with cudaGetSymbolAddress while that context is
+// current (the device's primary context for runtime-API callers) and caches
+// it under the context's unique ID, which CUDA never hands out twice in a
+// process. A context the host creates itself with the driver API, or the
+// primary context re-created after cudaDeviceReset, therefore resolves its
+// own address on its first call instead of reusing a stale one. That first
+// call per context should come before any stream capture.
 // All calls share the array and it keeps the previous call's contents, so
 // each call clears the accumulator planes it uses before the kernels run;
 // calls that overlap on the GPU (different streams, or different host
@@ -24,6 +29,8 @@
 // internal error a kernel flags is not reported back.
 #include "bm3d_device.cuh"
 #include "vsfeel_bm3d.h"
+
+#include <cuda.h>  // driver API types only; the calls are resolved at run time
 
 #include <algorithm>
 #include <cstdint>
@@ -42,30 +49,92 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratch
 
 namespace {
 
-constexpr int kMaxDevices = 64;
+// Resolved addresses, one per CUDA context seen (keyed by the context's
+// unique ID); the oldest entry is replaced when all are taken.
+constexpr int kCachedContexts = 64;
+
+struct CachedAddress {
+    unsigned long long ctx_id;
+    unsigned char* ptr;
+};
 
 std::mutex g_setup_lock;
-unsigned char* g_scratch_ptr[kMaxDevices] = {};
+CachedAddress g_cache[kCachedContexts] = {};
+int g_cache_used = 0, g_cache_next = 0;
 
-// The device address of the scratch array on the current device.
-int scratch_address(unsigned char** out) {
-    int dev = -1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+using CtxGetCurrentFn = CUresult (*)(CUcontext*);
+using CtxGetIdFn = CUresult (*)(CUcontext, unsigned long long*);
+
+// cuCtxGetCurrent and cuCtxGetId through the runtime's driver entry points,
+// so that the library does not link the driver library itself (it loads on
+// hosts without a GPU). Both exist from CUDA 12.0 on; without them every
+// call resolves the address afresh.
+struct DriverCalls {
+    CtxGetCurrentFn get_current = nullptr;
+    CtxGetIdFn get_id = nullptr;
+};
+
+const DriverCalls& driver_calls() {
+    static const DriverCalls calls = [] {
+        DriverCalls d;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault,
+                                             &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            d.get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+        fn = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            d.get_id = reinterpret_cast<CtxGetIdFn>(fn);
         cudaGetLastError();
-        return set_error(VSFEEL_E_CUDA, "no usable current CUDA device");
+        return d;
+    }();
+    return calls;
+}
+
+// The unique ID of the current context; false when there is none (nothing
+// has made a context current on this thread yet) or it cannot be read.
+bool current_context_id(unsigned long long* id) {
+    const DriverCalls& d = driver_calls();
+    if (!d.get_current || !d.get_id) return false;
+    CUcontext ctx = nullptr;
+    if (d.get_current(&ctx) != CUDA_SUCCESS || !ctx) return false;
+    return d.get_id(ctx, id) == CUDA_SUCCESS;
+}
+
+int resolve(unsigned char** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        cudaGetLastError();
+        return set_error(VSFEEL_E_CUDA, "could not resolve the scratch array's device address");
+    }
+    *out = static_cast<unsigned char*>(p);
+    return VSFEEL_OK;
+}
+
+// The device address of the scratch array in the current context.
+int scratch_address(unsigned char** out) {
+    unsigned long long id = 0;
+    if (!current_context_id(&id)) {
+        // no context current yet: the runtime call below makes the current
+        // device's primary context current, whose ID is then readable
+        const int rc = resolve(out);
+        if (rc != VSFEEL_OK || !current_context_id(&id)) return rc;
     }
     std::lock_guard<std::mutex> lk(g_setup_lock);
-    if (!g_scratch_ptr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return set_error(VSFEEL_E_CUDA, "could not resolve the scratch array's device address");
+    for (int i = 0; i < g_cache_used; ++i)
+        if (g_cache[i].ctx_id == id) {
+            *out = g_cache[i].ptr;
+            return VSFEEL_OK;
         }
-        g_scratch_ptr[dev] = static_cast<unsigned char*>(p);
-    }
-    *out = g_scratch_ptr[dev];
+    const int rc = resolve(out);
+    if (rc != VSFEEL_OK) return rc;
+    const int slot = g_cache_used < kCachedContexts ? g_cache_used++ : g_cache_next;
+    if (g_cache_used == kCachedContexts) g_cache_next = (slot + 1) % kCachedContexts;
+    g_cache[slot] = CachedAddress{id, *out};
     return VSFEEL_OK;
 }
 

@@ -55,6 +55,29 @@ def make_clip(nframes: int, height: int, width: int, sigma: float = 3.0, shift: 
     return out
 
 
+def make_clip_range(total: int, first: int, count: int, height: int, width: int,
+                    sigma: float = 3.0, shift: int = 3, seed: int = 0) -> np.ndarray:
+    """Frames first..first+count-1 of a `total`-frame clip, built without the
+    others: make_clip's canvas and per-frame offsets (the same numpy draws),
+    with each frame's noise from its own stream ``default_rng([seed, 2, f])``
+    so that any range of a long clip -- one rank's shard -- can be generated
+    alone. Returns float32 (count, height, width)."""
+    if not (0 <= first and count >= 0 and first + count <= total):
+        raise ValueError("frame range outside the clip")
+    rng = np.random.default_rng(seed)
+    canvas = clean_canvas(rng, height + 2 * shift, width + 2 * shift).astype(np.float32)
+    offsets = rng.integers(-shift, shift + 1, size=(total, 2))
+    out = np.empty((count, height, width), dtype=np.float32)
+    for i in range(count):
+        f = first + i
+        dx, dy = (int(v) for v in offsets[f])
+        out[i] = canvas[shift + dy:shift + dy + height, shift + dx:shift + dx + width]
+        if sigma > 0:
+            nrng = np.random.default_rng([seed, 2, f])
+            out[i] += nrng.standard_normal((height, width), dtype=np.float32) * np.float32(sigma / 255.0)
+    return out
+
+
 def make_chroma(nframes: int, height: int, width: int, seed: int = 0) -> np.ndarray:
     """A smooth random sinusoid field in [0, 1] for pass-through chroma planes."""
     rng = np.random.default_rng(seed + 7919)
