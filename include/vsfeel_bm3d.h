@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define VSFEEL_BM3D_ABI_VERSION 1
+#define VSFEEL_BM3D_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define VSFEEL_API __attribute__((visibility("default")))
@@ -280,8 +280,10 @@ VSFEEL_API int vsfeel_bm3d_backward(vsfeel_bm3d* ctx, const void* saved, const f
  * The class's work is captured once in a CUDA graph; a run replays the
  * classes' graphs one after another on the caller's stream. With
  * VSFEEL_BATCH_AUTOTUNE, vsfeel_bm3d_batch_create times every tile shape
- * that fits a class on one of its stacks and keeps the fastest; otherwise
- * the largest fitting shape is used. A class that no shape fits (radius >= 3,
+ * that fits a class (its reference blocks per CTA and the shape of the
+ * search region it stages) with 8 and with 16 lanes per reference block
+ * (threads per group) on one of its stacks, and keeps the fastest pair;
+ * otherwise the largest fitting shape with 8 lanes is used. A class that no shape fits (radius >= 3,
  * or windows too large) runs the direct-read kernels stack by stack inside
  * its graph.
  *
@@ -303,6 +305,8 @@ typedef struct vsfeel_bm3d_batch vsfeel_bm3d_batch;
 enum { VSFEEL_BATCH_AUTOTUNE = 1 };
 /* flags: use tile shape s for every class it fits (tests and tuning runs) */
 #define VSFEEL_BATCH_FORCE_SHAPE(s) ((((s) + 1) & 15) << 4)
+/* flags: use 8 or 16 lanes per reference block in every tiled class */
+#define VSFEEL_BATCH_FORCE_LANES(l) (((l) == 16 ? 2 : 1) << 8)
 
 /* Tile shapes of the tiled matcher, in reference blocks (x by y). */
 enum { VSFEEL_TILE_8X4 = 0, VSFEEL_TILE_16X2 = 1, VSFEEL_TILE_4X8 = 2, VSFEEL_TILE_8X2 = 3,
@@ -313,7 +317,9 @@ typedef struct vsfeel_bm3d_batch_class_info {
     int clips, stacks;
     int64_t tiles;          /* work-queue items per run                      */
     int tile_shape;         /* VSFEEL_TILE_*, or -1: direct-read kernels     */
-    double tuned_ms[VSFEEL_TILE_SHAPES]; /* autotuner's time per shape, or 0 */
+    double tuned_ms[VSFEEL_TILE_SHAPES]; /* autotuner's time per shape, 8 lanes, or 0 */
+    int lanes;              /* lanes per reference block of the tiled matcher */
+    double tuned_ms_16[VSFEEL_TILE_SHAPES]; /* the same with 16 lanes, or 0 */
 } vsfeel_bm3d_batch_class_info;
 
 VSFEEL_API int vsfeel_bm3d_batch_create(const vsfeel_bm3d_batch_clip* clips, int nclips, int device,

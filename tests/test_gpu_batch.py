@@ -68,12 +68,18 @@ def _run(batch):
     batch.finish()
 
 
-@pytest.mark.parametrize("mode", ["autotune", "default", "8x4", "16x2", "4x8", "8x2", "4x4"])
+@pytest.mark.parametrize("mode", ["autotune", "default", "8x4", "16x2", "4x8", "8x2", "4x4",
+                                  "8x4/16", "16x2/16", "4x4/16"])
 def test_batch_equals_plain_path_per_clip(mode):
+    """Every tile shape, with 8 lanes per reference block and (the /16
+    cases) 16 lanes per block in 512-thread CTAs."""
     src, dst = _inputs()
     kw = dict(autotune=mode == "autotune")
     if mode not in ("autotune", "default"):
-        kw["tile_shape"] = mode
+        shape, _, lanes = mode.partition("/")
+        kw["tile_shape"] = shape
+        if lanes:
+            kw["lanes"] = int(lanes)
     batch = Batch([(s, d, p) for s, d, (_, _, _, p) in zip(src, dst, CLIPS)], **kw)
     _run(batch)
     for i, (out, ref) in enumerate(zip(dst, _plain(src))):
@@ -92,9 +98,14 @@ def test_batch_classes_and_direct_read_fallback():
     assert keyed[(1, 4, 8, 2, 3)]["clips"] == 2           # clips 0 and 5 share a class
     assert keyed[(3, 4, 6, 2, 2)]["tile_shape"] == "direct"  # radius 3
     assert keyed[(1, 4, 8, 3, 3)]["tile_shape"] == "direct"  # seeds at (0, 0)
+    # the autotuner times every fitting shape with 8 and 16 lanes per block
+    # and keeps the fastest pair
     tuned = keyed[(2, 8, 12, 2, 4)]
     assert tuned["tile_shape"] in tuned["tuned_ms"]
-    assert tuned["tuned_ms"][tuned["tile_shape"]] == min(tuned["tuned_ms"].values())
+    assert set(tuned["tuned_ms"]) == set(tuned["tuned_ms_16"])
+    chosen = (tuned["tuned_ms"] if tuned["lanes"] == 8 else tuned["tuned_ms_16"])[tuned["tile_shape"]]
+    assert chosen == min(list(tuned["tuned_ms"].values()) + list(tuned["tuned_ms_16"].values()))
+    assert keyed[(3, 4, 6, 2, 2)]["lanes"] == 8   # direct-read classes report 8
     assert sum(c["stacks"] for c in classes) == sum(n for n, _, _, _ in CLIPS)
     assert batch.device_bytes > 0
 

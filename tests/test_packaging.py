@@ -91,7 +91,9 @@ def test_installed_wheel_loads_the_library(wheel, tmp_path):
     res = subprocess.run([sys.executable, "-c", code, str(target)], capture_output=True,
                          text=True, cwd=tmp_path, timeout=120)
     assert res.returncode == 0, res.stderr
-    assert res.stdout.strip() == "1"
+    from vsfeel import _lib
+
+    assert res.stdout.strip() == str(_lib.ABI_VERSION)
 
 
 def test_wheel_places_the_vapoursynth_plugin_where_vapoursynth_autoloads(plugin_wheel):

@@ -158,7 +158,9 @@ struct Class {
     std::vector<int> clips;
     std::vector<StackJob> jobs;
     int tile_shape = -1;
-    double tuned_ms[kTileShapes] = {};
+    int lanes = 8;                       // lanes per reference block of the matcher
+    double tuned_ms[kTileShapes] = {};   // autotuner's times, 8 lanes
+    double tuned_ms_16[kTileShapes] = {};  // and 16 lanes
     int64_t tiles = 0;
     size_t smem = 0;
     Dev<StackJob> d_jobs;
@@ -257,9 +259,11 @@ struct vsfeel_bm3d_batch {
 
 namespace {
 
-// Times every fitting tile shape on one stack of the class (no scatter) and
-// returns the fastest.
-int autotune(vsfeel_bm3d_batch* b, Class& cls, const StackJob& sample_in, const bool fits[]) {
+// Times every fitting tile shape with each allowed lane count (lanes_mask:
+// bit 0, 8 lanes; bit 1, 16 lanes) on one stack of the class (no scatter);
+// returns the fastest shape and sets cls.lanes to its lane count.
+int autotune(vsfeel_bm3d_batch* b, Class& cls, const StackJob& sample_in, const bool fits[],
+             int lanes_mask) {
     // the sample writes its match table into scratch of its own
     StackJob sample = sample_in;
     Dev<uint32_t> xy, zz;
@@ -297,23 +301,28 @@ int autotune(vsfeel_bm3d_batch* b, Class& cls, const StackJob& sample_in, const 
         const size_t smem = tile_smem_bytes(sample, TileShape(s), kTableOnly);
         const BatchWork work{job.p, first.p, 1, counter.p};
         const int grid = std::min(b->sms, tiles);
-        float best_rep = 0.0f;
-        for (int rep = 0; rep < 4; ++rep) {
-            check(cudaMemsetAsync(counter.p, 0, sizeof(int), cls.stream), "cudaMemsetAsync");
-            check(cudaEventRecord(e0, cls.stream), "cudaEventRecord");
-            check(launch_batch_tiles(work, TileShape(s), kTableOnly, 8, smem, grid, cls.stream),
-                  "autotune launch");
-            check(cudaEventRecord(e1, cls.stream), "cudaEventRecord");
-            if (wait_stream(cls.stream) != VSFEEL_OK)
-                throw Fail{VSFEEL_E_TIMEOUT, "timed out while autotuning"};
-            float ms = 0.0f;
-            check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-            if (rep > 0 && (rep == 1 || ms < best_rep)) best_rep = ms;  // first run warms up
-        }
-        cls.tuned_ms[s] = best_rep;
-        if (best < 0 || best_rep < best_ms) {
-            best = s;
-            best_ms = best_rep;
+        for (const int lanes : {8, 16}) {
+            if (!(lanes_mask & (lanes == 8 ? 1 : 2))) continue;
+            float best_rep = 0.0f;
+            for (int rep = 0; rep < 4; ++rep) {
+                check(cudaMemsetAsync(counter.p, 0, sizeof(int), cls.stream), "cudaMemsetAsync");
+                check(cudaEventRecord(e0, cls.stream), "cudaEventRecord");
+                check(launch_batch_tiles(work, TileShape(s), kTableOnly, lanes, smem, grid,
+                                         cls.stream),
+                      "autotune launch");
+                check(cudaEventRecord(e1, cls.stream), "cudaEventRecord");
+                if (wait_stream(cls.stream) != VSFEEL_OK)
+                    throw Fail{VSFEEL_E_TIMEOUT, "timed out while autotuning"};
+                float ms = 0.0f;
+                check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
+                if (rep > 0 && (rep == 1 || ms < best_rep)) best_rep = ms;  // first run warms up
+            }
+            (lanes == 8 ? cls.tuned_ms : cls.tuned_ms_16)[s] = best_rep;
+            if (best < 0 || best_rep < best_ms) {
+                best = s;
+                best_ms = best_rep;
+                cls.lanes = lanes;
+            }
         }
     }
     return best;
@@ -322,7 +331,7 @@ int autotune(vsfeel_bm3d_batch* b, Class& cls, const StackJob& sample_in, const 
 // Chooses the class's tile shape (autotuning it when asked) and cuts its
 // clips into chunks, recording each chunk's accumulator and match-table
 // needs; nothing is allocated for the class yet.
-void plan_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
+void plan_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced, int lanes_mask) {
     check(cudaStreamCreateWithFlags(&cls.stream, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaEventCreateWithFlags(&cls.done, cudaEventDisableTiming), "cudaEventCreate");
     // largest clips first: the queue's tail is made of small tiles
@@ -344,14 +353,21 @@ void plan_class(vsfeel_bm3d_batch* b, Class& cls, bool tune, int forced) {
                       tile_shape_fits(probe, TileShape(s), kTableOnly);
     }
     int shape = -1;
+    cls.lanes = (lanes_mask & 1) ? 8 : 16;
     if (forced >= 0 && forced < kTileShapes && fits[forced]) {
         shape = forced;
+        if (tune && lanes_mask == 3) {  // the shape is given: tune the lanes only
+            bool only[kTileShapes] = {};
+            only[forced] = true;
+            const Clip& big = b->clips[cls.clips.front()];
+            autotune(b, cls, b->make_job(big, nullptr, big.info.num_frames / 2, true), only, 3);
+        }
     } else if (tune) {
         const Clip& big = b->clips[cls.clips.front()];
         const StackJob sample = b->make_job(big, nullptr, big.info.num_frames / 2, true);
         bool any = false;
         for (int s = 0; s < kTileShapes; ++s) any = any || fits[s];
-        if (any) shape = autotune(b, cls, sample, fits);
+        if (any) shape = autotune(b, cls, sample, fits, lanes_mask);
     } else {
         const TileShape order[] = {kTile8x4, kTile16x2, kTile8x2, kTile4x4};
         for (TileShape s : order)
@@ -426,6 +442,7 @@ void finish_class(vsfeel_bm3d_batch* b, Class& cls) {
                 job.match_xy = b->match_xy.p + toff * 8;
                 job.match_z = b->match_z.p + toff;
                 if (shape >= 0) {
+                    job.lanes = cls.lanes;
                     cls.smem = std::max(cls.smem, tile_smem_bytes(job, TileShape(shape), kTableOnly));
                     const int64_t t = (int64_t)first.back() + tile_count(job, TileShape(shape));
                     const int64_t fi = (int64_t)ffirst.back() + filter_items((int)nb);
@@ -486,7 +503,8 @@ void finish_class(vsfeel_bm3d_batch* b, Class& cls) {
             const BatchWork work{cls.d_jobs.p + ch.job0, cls.d_tile_first.p + ch.first_off, ch.njobs,
                                  cls.counter.p + k};
             const int grid = std::min(b->sms, ch.tiles);
-            err = launch_batch_tiles(work, TileShape(shape), kTableOnly, 8, cls.smem, grid, cls.stream);
+            err = launch_batch_tiles(work, TileShape(shape), kTableOnly, cls.lanes, cls.smem, grid,
+                                     cls.stream);
             const FilterBatch fw{cls.d_jobs.p + ch.job0, cls.d_filter_first.p + ch.ffirst_off,
                                  ch.njobs};
             if (err == cudaSuccess) err = launch_filter_batch(fw, ch.filter_items, cls.stream);
@@ -575,8 +593,11 @@ int vsfeel_bm3d_batch_create(const vsfeel_bm3d_batch_clip* clips, int nclips, in
         check(cudaMemset(b->status.p, 0, sizeof(int)), "cudaMemset");
         check(cudaEventCreateWithFlags(&b->start, cudaEventDisableTiming), "cudaEventCreate");
         const int forced = ((flags >> 4) & 15) - 1;
+        const int force_lanes = (flags >> 8) & 15;  // 0: tune or default; 1: 8; 2: 16
+        const int lanes_mask = force_lanes == 1 ? 1 : (force_lanes == 2 ? 2 : 3);
         for (Class& cls : b->classes)
-            plan_class(b, cls, (flags & VSFEEL_BATCH_AUTOTUNE) != 0, forced);
+            plan_class(b, cls, (flags & VSFEEL_BATCH_AUTOTUNE) != 0, forced,
+                       (flags & VSFEEL_BATCH_AUTOTUNE) || force_lanes ? lanes_mask : 1);
         b->acc.alloc(b->acc_need);
         b->match_xy.alloc(b->table_need * 8);
         b->match_z.alloc(b->table_need);
@@ -658,7 +679,11 @@ int vsfeel_bm3d_batch_class(const vsfeel_bm3d_batch* b, int index,
     info->stacks = (int)c.jobs.size();
     info->tiles = c.tiles;
     info->tile_shape = c.tile_shape;
-    for (int s = 0; s < kTileShapes && s < VSFEEL_TILE_SHAPES; ++s) info->tuned_ms[s] = c.tuned_ms[s];
+    info->lanes = c.tile_shape >= 0 ? c.lanes : 8;
+    for (int s = 0; s < kTileShapes && s < VSFEEL_TILE_SHAPES; ++s) {
+        info->tuned_ms[s] = c.tuned_ms[s];
+        info->tuned_ms_16[s] = c.tuned_ms_16[s];
+    }
     return VSFEEL_OK;
 }
 

@@ -48,7 +48,7 @@ EXPORTS = (
     "vsfeel_bm3d_abi_version",
 )
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 E_ARG = -1
@@ -141,6 +141,8 @@ class BatchClassInfo(ctypes.Structure):
         ("tiles", ctypes.c_int64),
         ("tile_shape", ctypes.c_int),
         ("tuned_ms", ctypes.c_double * len(TILE_SHAPES)),
+        ("lanes", ctypes.c_int),
+        ("tuned_ms_16", ctypes.c_double * len(TILE_SHAPES)),
     ]
 
 

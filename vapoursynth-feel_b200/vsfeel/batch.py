@@ -18,11 +18,12 @@ from . import Error, _lib, _make_args
 
 class Batch:
     def __init__(self, clips, device: int = 0, autotune: bool = True,
-                 tile_shape: str | None = None):
+                 tile_shape: str | None = None, lanes: int | None = None):
         """clips: sequence of (src, dst, params) with params the BM3Dv2
         keyword arguments (sigma, block_step, bm_range, radius, ps_num,
         ps_range, extractor_exp). tile_shape ("8x4", "16x2", "4x8", "8x2",
-        "4x4") forces that shape on every class it fits."""
+        "4x4") forces that shape on every class it fits; lanes (8 or 16)
+        forces the lanes per reference block of every tiled class."""
         import torch
 
         self.lib = _lib.load()
@@ -53,6 +54,10 @@ class Batch:
         flags = _lib.BATCH_AUTOTUNE if autotune else 0
         if tile_shape is not None:
             flags |= ((_lib.TILE_SHAPES.index(tile_shape) + 1) & 15) << 4
+        if lanes is not None:
+            if lanes not in (8, 16):
+                raise Error("BM3D: lanes must be 8 or 16")
+            flags |= (2 if lanes == 16 else 1) << 8
         rc = self.lib.vsfeel_bm3d_batch_create(arr, len(clips), self.device, flags,
                                                ctypes.byref(handle))
         if rc != _lib.OK:
@@ -93,8 +98,11 @@ class Batch:
                 "ps_num": info.ps_num, "ps_range": info.ps_range, "clips": info.clips,
                 "stacks": info.stacks, "tiles": info.tiles,
                 "tile_shape": _lib.TILE_SHAPES[shape] if shape >= 0 else "direct",
+                "lanes": info.lanes,
                 "tuned_ms": {_lib.TILE_SHAPES[s]: info.tuned_ms[s]
                              for s in range(len(_lib.TILE_SHAPES)) if info.tuned_ms[s] > 0},
+                "tuned_ms_16": {_lib.TILE_SHAPES[s]: info.tuned_ms_16[s]
+                                for s in range(len(_lib.TILE_SHAPES)) if info.tuned_ms_16[s] > 0},
             })
         return out
 
