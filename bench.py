@@ -415,6 +415,62 @@ def time_frame_requests(luma, u, v, dev_index, passes, threads):
             "passes": passes}
 
 
+# Small workloads for ncu captures (a few GB of device memory at most, so
+# that a capture of one launch ends quickly): each runs its path once per
+# step, device-resident, and prints one line with the step time.
+PROFILE_CASES = {
+    # the radius >= 3 exact search with the 3840x2160 workload's arguments,
+    # on 1080p frames (one stack per match launch)
+    "exact_1920x1080x9_r4": dict(frames=9, height=HEIGHT, width=WIDTH, shift=6, seed=4100,
+                                 params=dict(sigma=8.0, block_step=4, bm_range=16, radius=4,
+                                             ps_num=4, ps_range=7, extractor_exp=2)),
+    # the batched form on a mixed handful of clips (one persistent launch per
+    # class chunk)
+    "batched_small": None,
+}
+
+
+def run_profile_case(torch, dev, name, steps, warmup):
+    from vsfeel.synthetic import make_clip_device
+
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if name == "batched_small":
+        from vsfeel.batch import Batch
+
+        spec = [(4, 1080, 1920, dict(sigma=3.0, block_step=4, bm_range=16, radius=2, ps_num=2,
+                                     ps_range=7))] * 2 + \
+               [(8, 360, 640, dict(sigma=5.0, block_step=8, bm_range=16, radius=1, ps_num=2,
+                                   ps_range=7))] * 4
+        src = [make_clip_device(n, h, w, p["sigma"], shift=4, seed=4200 + i, device=dev)
+               for i, (n, h, w, p) in enumerate(spec)]
+        dst = [torch.empty_like(x) for x in src]
+        batch = Batch([(x, y, p) for x, y, (_, _, _, p) in zip(src, dst, spec)],
+                      device=dev.index or 0, autotune=False)
+        run = batch.run
+        px = sum(n * h * w for n, h, w, _ in spec)
+    else:
+        wl = PROFILE_CASES[name]
+        x = make_clip_device(wl["frames"], wl["height"], wl["width"], sigma=wl["params"]["sigma"],
+                             shift=wl["shift"], seed=wl["seed"], device=dev)
+        from vsfeel.autograd import Denoiser
+
+        out = torch.empty_like(x)
+        den = Denoiser(x.shape, dev.index or 0, **wl["params"])
+        run = lambda: den.plain(x, out)  # noqa: E731
+        px = x.numel()
+    for _ in range(warmup):
+        run()
+    torch.cuda.synchronize()
+    a.record()
+    for _ in range(steps):
+        run()
+    b.record()
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / max(steps, 1)
+    return {"profile_case": name, "ms_per_step": ms, "mpx_s": px / ms / 1e3, "steps": steps,
+            "warmup": warmup}
+
+
 def run_reference(args) -> int:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -497,9 +553,19 @@ def main() -> int:
                          "profiling target) and print its line")
     ap.add_argument("--case-frames", type=int, default=None,
                     help="frames of the --case clip (default: the workload's)")
+    ap.add_argument("--profile-case", choices=sorted(PROFILE_CASES),
+                    help="only run this small profiling workload and print its line")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_case:
+        import torch
+
+        dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+        torch.cuda.set_device(dev)
+        print(json.dumps(run_profile_case(torch, dev, args.profile_case, args.steps, args.warmup)),
+              flush=True)
+        return 0
     if args.case:
         import torch
 
