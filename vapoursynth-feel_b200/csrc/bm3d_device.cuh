@@ -134,9 +134,12 @@ inline int filter_items(int nblocks) { return (nblocks + 15) / 16; }
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream);
 cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream);
 cudaError_t launch_normalize_batch(const NormalizeBatch& work, int total_tiles, cudaStream_t stream);
-// The normaliser's tile: 8 rows (one warp each) of 120 pixels (30 lanes of
+// The normaliser's tile: 2 rows (one warp each) of 120 pixels (30 lanes of
 // 4 pixels, the warp's other 2 lanes reading the 8-column halo on the left).
-constexpr int kNormTileW = 120, kNormTileH = 8;
+// Its 64-thread CTAs are small enough (80 registers a thread) to sit on an SM
+// beside a matcher CTA and a filter CTA, so that normalisations overlap the
+// next stack's matching instead of waiting for the matcher grid's tail.
+constexpr int kNormTileW = 120, kNormTileH = 2;
 inline int normalize_tiles(int width, int height) {
     return ((width + kNormTileW - 1) / kNormTileW) * ((height + kNormTileH - 1) / kNormTileH);
 }

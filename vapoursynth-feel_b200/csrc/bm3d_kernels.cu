@@ -306,8 +306,11 @@ __device__ __forceinline__ void normalize_tile(const NormalizeJob& job, int tx0,
     const bool has_px = lane >= 2 && x0 < job.width;
     const bool col_ok = col >= 0 && col + 3 < job.src_pitch;
     double acc[4] = {0.0, 0.0, 0.0, 0.0}, acw[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll 1
-    for (int i = 0; i < job.tw; ++i) {
+    // slices indexed statically (the slice pointers stay in the parameter
+    // space), in the reference's order
+#pragma unroll
+    for (int i = 0; i < kMaxTW; ++i) {
+        if (i >= job.tw) break;
         const float* org = job.num[i] + job.den_offset;
         float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
@@ -352,7 +355,7 @@ __device__ __forceinline__ void normalize_tile(const NormalizeJob& job, int tx0,
     }
 }
 
-__global__ void __launch_bounds__(256) bm3d_normalize_kernel(const NormalizeJob job) {
+__global__ void __launch_bounds__(32 * kNormTileH) bm3d_normalize_kernel(const NormalizeJob job) {
     normalize_tile(job, blockIdx.x * kNormTileW, blockIdx.y * kNormTileH);
 }
 
@@ -381,8 +384,8 @@ __global__ void __launch_bounds__(128) bm3d_filter_batch_kernel(const FilterBatc
     filter_group<false>(job, b, valid, mxy, job.match_z[b], sub, buf);
 }
 
-// Batched form: one CTA per 128x8 tile of one output frame.
-__global__ void __launch_bounds__(256) bm3d_normalize_batch_kernel(const NormalizeBatch work) {
+// Batched form: one CTA per normaliser tile of one output frame.
+__global__ void __launch_bounds__(32 * kNormTileH) bm3d_normalize_batch_kernel(const NormalizeBatch work) {
     const int item = blockIdx.x;
     int lo = 0, hi = work.njobs - 1;
     while (lo < hi) {  // last job whose first tile is <= item
@@ -537,7 +540,7 @@ cudaError_t launch_filter_batch(const FilterBatch& work, int total_items, cudaSt
 cudaError_t launch_normalize_batch(const NormalizeBatch& work, int total_tiles,
                                    cudaStream_t stream) {
     if (total_tiles <= 0) return cudaSuccess;
-    bm3d_normalize_batch_kernel<<<total_tiles, 256, 0, stream>>>(work);
+    bm3d_normalize_batch_kernel<<<total_tiles, 32 * kNormTileH, 0, stream>>>(work);
     return cudaGetLastError();
 }
 
@@ -552,7 +555,7 @@ cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream) {
 
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream) {
     dim3 grid((job.width + kNormTileW - 1) / kNormTileW, (job.height + kNormTileH - 1) / kNormTileH);
-    bm3d_normalize_kernel<<<grid, 256, 0, stream>>>(job);
+    bm3d_normalize_kernel<<<grid, 32 * kNormTileH, 0, stream>>>(job);
     return cudaGetLastError();
 }
 
