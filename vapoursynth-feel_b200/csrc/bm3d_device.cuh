@@ -129,8 +129,11 @@ struct FilterBatch {
     const int* group_first;
     int njobs;
 };
-cudaError_t launch_filter_batch(const FilterBatch& work, int total_items, cudaStream_t stream);
-inline int filter_items(int nblocks) { return (nblocks + 15) / 16; }
+// groups: blocks per item (and CTA): 16, or 8 for CTAs small enough to run
+// beside a matcher CTA
+cudaError_t launch_filter_batch(const FilterBatch& work, int total_items, int groups,
+                                cudaStream_t stream);
+inline int filter_items(int nblocks, int groups = 16) { return (nblocks + groups - 1) / groups; }
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream);
 cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream);
 cudaError_t launch_normalize_batch(const NormalizeBatch& work, int total_tiles, cudaStream_t stream);

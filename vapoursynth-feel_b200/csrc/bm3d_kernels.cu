@@ -359,9 +359,10 @@ __global__ void __launch_bounds__(32 * kNormTileH) bm3d_normalize_kernel(const N
     normalize_tile(job, blockIdx.x * kNormTileW, blockIdx.y * kNormTileH);
 }
 
-// Batched form: the filter of 16 blocks of one stack per CTA.
-__global__ void __launch_bounds__(128) bm3d_filter_batch_kernel(const FilterBatch work) {
-    __shared__ float smem[kFilterGroupsPerCta * kGroupStride];
+// Batched form: the filter of kGroups blocks of one stack per CTA.
+template <int kGroups>
+__global__ void __launch_bounds__(kGroups * 8) bm3d_filter_batch_kernel(const FilterBatch work) {
+    __shared__ float smem[kGroups * kGroupStride];
     const int item = blockIdx.x;
     int lo = 0, hi = work.njobs - 1;
     while (lo < hi) {  // last job whose first item is <= item
@@ -375,7 +376,7 @@ __global__ void __launch_bounds__(128) bm3d_filter_batch_kernel(const FilterBatc
     const int sub = threadIdx.x & 7;
     float* buf = smem + (threadIdx.x >> 3) * kGroupStride;
     const int nblocks = job.nbx * job.nby;
-    const int gblock = (item - work.group_first[lo]) * 16 + (threadIdx.x >> 3);
+    const int gblock = (item - work.group_first[lo]) * kGroups + (threadIdx.x >> 3);
     const bool valid = gblock < nblocks;
     const int b = valid ? gblock : nblocks - 1;
     const uint4 m0 = reinterpret_cast<const uint4*>(job.match_xy + (size_t)b * 8)[0];
@@ -531,9 +532,13 @@ cudaError_t launch_filter_beside_match(const StackJob& job, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-cudaError_t launch_filter_batch(const FilterBatch& work, int total_items, cudaStream_t stream) {
+cudaError_t launch_filter_batch(const FilterBatch& work, int total_items, int groups,
+                                cudaStream_t stream) {
     if (total_items <= 0) return cudaSuccess;
-    bm3d_filter_batch_kernel<<<total_items, kThreads, 0, stream>>>(work);
+    if (groups == 8)
+        bm3d_filter_batch_kernel<8><<<total_items, 64, 0, stream>>>(work);
+    else
+        bm3d_filter_batch_kernel<16><<<total_items, 128, 0, stream>>>(work);
     return cudaGetLastError();
 }
 
