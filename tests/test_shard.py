@@ -100,3 +100,39 @@ def test_world_size_two_gloo(tmp_path):
     full = np.load(out)
     frames = make_clip(7, 40, 48, sigma=PARAMS["sigma"], shift=2, seed=5)
     assert np.array_equal(full, Oracle().bm3d(frames, Params(**PARAMS), nthreads=2))
+
+
+def test_frame_ranges_generate_alone_and_agree_with_the_whole_clip():
+    """The multi-GPU bench builds each rank's sub-clip alone
+    (make_clip_range); every range must equal the same frames of the whole
+    clip, and its clean frames make_clip's."""
+    from vsfeel.synthetic import make_clip_range
+
+    total = 12
+    whole = make_clip_range(total, 0, total, 40, 56, sigma=3.0, shift=4, seed=2000)
+    for sh in shard.plan(total, 3, 2):
+        part = make_clip_range(total, sh.in_first, sh.in_count, 40, 56, sigma=3.0, shift=4,
+                               seed=2000)
+        assert np.array_equal(part, whole[sh.in_first:sh.in_last + 1])
+    clean = make_clip(total, 40, 56, sigma=0.0, shift=4, seed=2000)
+    assert np.array_equal(make_clip_range(total, 0, total, 40, 56, sigma=0.0, shift=4, seed=2000),
+                          clean)
+    with pytest.raises(ValueError):
+        make_clip_range(total, 10, 5, 40, 56)
+
+
+@pytest.mark.parametrize("world,r", [(1, 2), (2, 2), (4, 2), (8, 2), (8, 4)])
+def test_halo_recompute_fraction_of_the_sharded_bench(world, r):
+    """Stacks a sharded run computes beyond one per output frame: each
+    interior side of a shard adds r stacks (its halo outputs' stacks), so
+    for 32 outputs per rank the fraction is 2r(N-1)/(32N)."""
+    nfr = 32
+    plans = shard.plan(nfr * world, world, r)
+
+    def stacks(s):
+        lo = max(s.local_first - r, 0)
+        hi = min(s.local_first + s.out_count - 1 + r, s.in_count - 1)
+        return hi - lo + 1
+
+    frac = sum(stacks(s) for s in plans) / (nfr * world) - 1.0
+    assert abs(frac - 2 * r * (world - 1) / (nfr * world)) < 1e-12

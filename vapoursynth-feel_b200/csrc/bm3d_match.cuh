@@ -677,24 +677,14 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
     const int sub = threadIdx.x & (kLanes - 1);
     int total_rows = 0;
     for (int i = 0; i < nwin; ++i) total_rows += wins[i].h;
-    // the exact scan keeps 8 column sums per row: 2 or 3 rows per lane,
-    // whichever leaves the 8 lanes less work in all. A step of 3 rows costs
-    // about 1.65 steps of 2 on B200 (measured at 1080p r3 and 4K r4: the
-    // 3-row form runs at the register limit)
+    // the exact scan keeps 8 column sums per row: 2 rows per lane, so that
+    // its kernel fits 128 registers and two CTAs (16 warps) share an SM
+    // (11.7% faster per 1080p r4 stack than 2 or 3 rows at one CTA per SM)
     int K;
-    if (kExact) {
-        constexpr int kStep2 = 20, kStep3 = 33;
-        int t2 = 0, t3 = 0;
-        for (int i = 0; i < nwin; ++i) {
-            t2 += (wins[i].h + 1) / 2;
-            t3 += (wins[i].h + 2) / 3;
-        }
-        const int c2 = (t2 + 7) / 8 * kStep2;
-        const int c3 = (t3 + 7) / 8 * kStep3;
-        K = warp_max(c3 < c2 ? 3 : 2);
-    } else {
+    if (kExact)
+        K = 2;
+    else
         K = warp_max(rows_per_lane<kLanes>(total_rows));
-    }
     int ntasks = 0;
     for (int i = 0; i < nwin; ++i) ntasks += qdiv<kExact>(wins[i].h + K - 1, K);
     const int rounds = warp_max((ntasks + kLanes - 1) / kLanes);
@@ -729,11 +719,8 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
         }
         const int jcount = warp_max(has ? win.rw + 7 : 8);
         if (kExact) {
-            switch (K) {
-                // E: the block interleaved by column pairs (see scan_chunk_exact)
-                case 2: scan_chunk_exact<2>(reg, E, win, r0, nrows, jcount, top); break;
-                default: scan_chunk_exact<3>(reg, E, win, r0, nrows, jcount, top); break;
-            }
+            // E: the block interleaved by column pairs (see scan_chunk_exact)
+            scan_chunk_exact<2>(reg, E, win, r0, nrows, jcount, top);
         } else if (kLanes == 16) {
             if (K == 2)
                 scan_chunk<2>(reg, cur_s, c7, win, r0, nrows, jcount, E, lb);
@@ -1118,9 +1105,10 @@ __global__ void __launch_bounds__(TX * TY * kLanes, 1) bm3d_match_sliding_kernel
     match_tile<TX, TY, kMode, false, kLanes>(job, blockIdx.x, smem_raw);
 }
 
-// radius >= 3: the same tile body with the exact scan (match table only)
+// radius >= 3: the same tile body with the exact scan (match table only);
+// two CTAs per SM (128 registers, ~100 KB of shared memory each)
 template <int TX, int TY>
-__global__ void __launch_bounds__(TX * TY * 8, 1) bm3d_match_exact_kernel(const StackJob job) {
+__global__ void __launch_bounds__(TX * TY * 8, 2) bm3d_match_exact_kernel(const StackJob job) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     match_tile<TX, TY, kTableOnly, true>(job, blockIdx.x, smem_raw);
 }
