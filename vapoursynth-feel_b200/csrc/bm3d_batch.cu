@@ -17,7 +17,7 @@
 //     their 32x8 tiles;
 //   * a match table per stack;
 //   * a CUDA graph: per chunk, clear its accumulators, the persistent
-//     matching launch (one CTA per SM) over its queue, one filter launch over
+//     matching launch (as many CTAs as the SMs hold) over its queue, one filter launch over
 //     every block of its stacks, one normalise launch. (The
 //     filter stays a separate kernel: inside the matcher's one CTA per SM
 //     its atomics run slower than at the filter kernel's occupancy.)
@@ -315,9 +315,12 @@ int autotune(vsfeel_bm3d_batch* b, Class& cls, const StackJob& sample_in, const 
         check(cudaMemcpy(first.p, h_first, sizeof(h_first), cudaMemcpyHostToDevice), "cudaMemcpy");
         const size_t smem = tile_smem_bytes(sample, TileShape(s), kTableOnly);
         const BatchWork work{job.p, first.p, 1, counter.p};
-        const int grid = std::min(b->sms, tiles);
         for (const int lanes : {8, 16}) {
             if (!(lanes_mask & (lanes == 8 ? 1 : 2))) continue;
+            // as many CTAs as the SMs hold at once (two per SM for the
+            // 16-block shapes, whose plans take ~115 KB)
+            const int grid =
+                std::min(b->sms * batch_ctas_per_sm(TileShape(s), kTableOnly, lanes, smem), tiles);
             float best_rep = 0.0f;
             for (int rep = 0; rep < 4; ++rep) {
                 check(cudaMemsetAsync(counter.p, 0, sizeof(int), cls.stream), "cudaMemsetAsync");
@@ -536,6 +539,9 @@ void finish_class(vsfeel_bm3d_batch* b, Class& cls) {
         }
     }
     cudaStream_t ms = cls.stream, fs = two ? cls.stream2 : cls.stream;
+    // the persistent grid: as many CTAs as the SMs hold at once
+    const int ctas_per_sm =
+        shape >= 0 ? batch_ctas_per_sm(TileShape(shape), kTableOnly, cls.lanes, cls.smem) : 1;
     check(cudaStreamBeginCapture(ms, cudaStreamCaptureModeRelaxed), "capture");
     cudaError_t err = cudaMemsetAsync(cls.counter.p, 0, sizeof(int) * cls.chunks.size(), ms);
     if (two && err == cudaSuccess) {
@@ -552,7 +558,7 @@ void finish_class(vsfeel_bm3d_batch* b, Class& cls) {
         if (err == cudaSuccess && shape >= 0) {
             const BatchWork work{cls.d_jobs.p + ch.job0, cls.d_tile_first.p + ch.first_off, ch.njobs,
                                  cls.counter.p + k};
-            const int grid = std::min(b->sms, ch.tiles);
+            const int grid = std::min(b->sms * ctas_per_sm, ch.tiles);
             err = launch_batch_tiles(work, TileShape(shape), kTableOnly, cls.lanes, cls.smem, grid,
                                      ms);
             if (err == cudaSuccess && two) {

@@ -117,6 +117,8 @@ size_t tile_smem_bytes(const StackJob& job, TileShape shape, TileMode mode);
 int tile_count(const StackJob& job, TileShape shape);
 cudaError_t launch_match_tiles(const StackJob& job, TileShape shape, TileMode mode,
                                cudaStream_t stream);
+// CTAs of the persistent kernel one SM holds at once (its grid: this many per SM)
+int batch_ctas_per_sm(TileShape shape, TileMode mode, int lanes, size_t smem);
 // mode: kTableOnly or kFused; lanes: 8, or 16 with kTableOnly
 cudaError_t launch_batch_tiles(const BatchWork& work, TileShape shape, TileMode mode, int lanes,
                                size_t smem, int grid, cudaStream_t stream);

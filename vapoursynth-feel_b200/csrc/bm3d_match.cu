@@ -11,7 +11,8 @@ namespace vsfeel {
     size_t tile_plan_bytes_##TX##x##TY(const StackJob& job, TileMode mode);                   \
     cudaError_t launch_tiles_##TX##x##TY(const StackJob& job, TileMode mode, cudaStream_t s); \
     cudaError_t launch_batch_##TX##x##TY(const BatchWork& work, TileMode mode, int lanes,     \
-                                         size_t smem, int grid, cudaStream_t s);
+                                         size_t smem, int grid, cudaStream_t s);            \
+    int batch_ctas_per_sm_##TX##x##TY(TileMode mode, int lanes, size_t smem);
 VSFEEL_TILE_DECL(8, 4)
 VSFEEL_TILE_DECL(16, 2)
 VSFEEL_TILE_DECL(4, 8)
@@ -93,6 +94,16 @@ cudaError_t launch_match_tiles(const StackJob& job, TileShape shape, TileMode mo
         case kTile4x8: return launch_tiles_4x8(job, mode, stream);
         case kTile8x2: return launch_tiles_8x2(job, mode, stream);
         default: return launch_tiles_4x4(job, mode, stream);
+    }
+}
+
+int batch_ctas_per_sm(TileShape shape, TileMode mode, int lanes, size_t smem) {
+    switch (shape) {
+        case kTile8x4: return batch_ctas_per_sm_8x4(mode, lanes, smem);
+        case kTile16x2: return batch_ctas_per_sm_16x2(mode, lanes, smem);
+        case kTile4x8: return batch_ctas_per_sm_4x8(mode, lanes, smem);
+        case kTile8x2: return batch_ctas_per_sm_8x2(mode, lanes, smem);
+        default: return batch_ctas_per_sm_4x4(mode, lanes, smem);
     }
 }
 

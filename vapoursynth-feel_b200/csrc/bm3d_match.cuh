@@ -1199,6 +1199,26 @@ cudaError_t launch_grid_mode(const StackJob& job, TileMode mode, cudaStream_t st
     }
 }
 
+// CTAs of the persistent kernel that one SM holds at once (with `smem`
+// bytes of dynamic shared memory): the persistent grid is this many per SM.
+template <int TX, int TY>
+int batch_ctas_per_sm(TileMode mode, int lanes, size_t smem) {
+    auto* fn = mode == kFused ? bm3d_batch_tile_kernel<TX, TY, kFused>
+                              : (lanes == 16 ? bm3d_batch_tile_kernel<TX, TY, kTableOnly, 16>
+                                             : bm3d_batch_tile_kernel<TX, TY, kTableOnly>);
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, TX * TY * lanes, smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    return n > 0 ? n : 1;
+}
+
 template <int TX, int TY>
 cudaError_t launch_batch(const BatchWork& work, TileMode mode, int lanes, size_t smem, int grid,
                          cudaStream_t stream) {

@@ -20,4 +20,8 @@ cudaError_t launch_batch_16x2(const BatchWork& work, TileMode mode, int lanes, s
     return launch_batch<16, 2>(work, mode, lanes, smem, grid, s);
 }
 
+int batch_ctas_per_sm_16x2(TileMode mode, int lanes, size_t smem) {
+    return batch_ctas_per_sm<16, 2>(mode, lanes, smem);
+}
+
 }  // namespace vsfeel

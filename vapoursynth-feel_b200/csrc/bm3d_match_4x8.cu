@@ -20,4 +20,8 @@ cudaError_t launch_batch_4x8(const BatchWork& work, TileMode mode, int lanes, si
     return launch_batch<4, 8>(work, mode, lanes, smem, grid, s);
 }
 
+int batch_ctas_per_sm_4x8(TileMode mode, int lanes, size_t smem) {
+    return batch_ctas_per_sm<4, 8>(mode, lanes, smem);
+}
+
 }  // namespace vsfeel
