@@ -388,3 +388,22 @@ def test_sixteen_lanes_per_block_vs_oracle(kw, shape, monkeypatch, oracle_lib):
         assert np.array_equal(out, expected)
     else:
         assert float(np.abs(out.astype(np.float64) - expected).max()) <= TYPICAL_TOL
+
+
+def test_autotuned_and_default_contexts_agree(monkeypatch, oracle_lib):
+    """The plain path's autotuner (first call: every fitting tile shape and
+    lane count timed on the first stack) changes only the speed: match
+    tables bit-exact against the oracle and outputs equal to the untuned
+    context's within the float-atomic bar."""
+    kw = dict(sigma=5.0, block_step=4, bm_range=12, radius=1, ps_num=2, ps_range=5)
+    frames = make_clip(6, 256, 256, sigma=5.0, shift=3, seed=71)
+    p = Params(**kw)
+    monkeypatch.setenv("VSFEEL_AUTOTUNE", "0")
+    plain = _node(frames, **kw).output()
+    monkeypatch.setenv("VSFEEL_AUTOTUNE", "1")
+    node = _node(frames, **kw)
+    tuned = node.output()
+    assert float(np.abs(tuned - plain).max()) <= TYPICAL_TOL
+    assert float(np.abs(tuned.astype(np.float64) - oracle_lib.bm3d(frames, p)).max()) <= TYPICAL_TOL
+    for m in (0, 3, 5):
+        assert np.array_equal(_cuda_tables(frames, p, [m])[m], oracle_lib.matches(frames, p, m))

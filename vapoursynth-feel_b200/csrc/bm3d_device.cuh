@@ -42,6 +42,8 @@ struct StackJob {
     int* status;                       // device word, set nonzero on an internal error
     int lanes;                         // tiled sliding matcher: lanes per block, 8 (also 0)
                                        // or 16 (table mode only, 512-thread CTAs)
+    int tile_shape_plus1;              // 1 + TileShape the table-mode matcher uses (when it
+                                       // fits); 0: the default order
     int probe_tile;                    // test hook: 1 + index of a tile whose staged-region
                                        // check reports a window outside (the tile sets
                                        // *status and scans nothing); 0 = none

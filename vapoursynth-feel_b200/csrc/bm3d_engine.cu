@@ -300,6 +300,57 @@ struct vsfeel_bm3d {
     // 8 (256-thread CTAs) or 16 (512-thread CTAs, twice the warps per SM at
     // the same shared memory). VSFEEL_MATCH_LANES overrides the default.
     int match_lanes = 8;
+    // The plain path's autotuner (VSFEEL_AUTOTUNE=0 turns it off): on the
+    // first call that launches stacks, one table-only matching launch of the
+    // call's first stack per fitting (tile shape, lanes) pair, timed with
+    // events; a pair replaces the default only when it is at least 2% faster.
+    // Every pair gives the same match table.
+    bool autotune = true;
+    int tuned = 0;           // 0: not tuned yet; 1: tuned
+    int tuned_shape_plus1 = 0;
+    void ensure_tuned(const StackJob& sample_in, cudaStream_t st) {
+        if (tuned || !autotune || sample_in.radius >= 3 || sample_in.wiener) {
+            tuned = 1;
+            return;
+        }
+        tuned = 1;
+        const int def = default_tile_shape(sample_in, kTableOnly);
+        if (def < 0) return;
+        StackJob sample = sample_in;
+        for (int z = 0; z < kMaxTW; ++z) sample.slice_dst[z] = nullptr;  // table only
+        cudaEvent_t e0 = next_event(), e1 = next_event();
+        auto time_one = [&](int shape, int lanes) -> float {
+            sample.tile_shape_plus1 = shape + 1;
+            sample.lanes = lanes;
+            float best = -1.0f;
+            for (int rep = 0; rep < 3; ++rep) {
+                VSF_CUDA(cudaEventRecord(e0, st));
+                VSF_CUDA(launch_match(sample, st));
+                launches += 1;
+                VSF_CUDA(cudaEventRecord(e1, st));
+                if (wait_event(e1, timeout_ms()) != VSFEEL_OK) return -1.0f;
+                float ms = 0.0f;
+                VSF_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+                if (rep > 0 && (best < 0.0f || ms < best)) best = ms;  // the first warms up
+            }
+            return best;
+        };
+        const float base = time_one(def, 8);
+        if (base <= 0.0f) return;
+        float best = base;
+        for (int s = 0; s < kTileShapes; ++s) {
+            if (!tile_shape_fits(sample, TileShape(s), kTableOnly)) continue;
+            for (const int lanes : {8, 16}) {
+                if (s == def && lanes == 8) continue;
+                const float t = time_one(s, lanes);
+                if (t > 0.0f && t < best && t < 0.98f * base) {
+                    best = t;
+                    tuned_shape_plus1 = s + 1;
+                    match_lanes = lanes;
+                }
+            }
+        }
+    }
 
     DevBuf<float> ring;       // (2r+1) slots x TW x {num, den} planes
     DevBuf<uint32_t> match_xy;
@@ -558,6 +609,7 @@ struct vsfeel_bm3d {
         job.status = status_word();
         job.probe_tile = probe_tile_from_env();
         job.lanes = match_lanes;
+        job.tile_shape_plus1 = tuned_shape_plus1;
         return job;
     }
 
@@ -669,6 +721,14 @@ struct vsfeel_bm3d {
         int zeroed = first - 1;     // highest output whose slot is zeroed
         int finished = first - 1;   // highest output normalised
         const bool two = overlap && !fused;
+        if (!tuned) {
+            // the first stack's frames must be resident: the host path
+            // uploads them just before the stack that needs them
+            if (before_stack) (*before_stack)(m_lo, st);
+            ensure_tuned(stack_job(m_lo, frame_ptr, in_pitch, first, last, saved, input_ptr, nullptr,
+                                   match_xy.p, match_z.p),
+                         st);
+        }
         cudaStream_t fs = st;  // filter, slot clearing, normalisation
         cudaStream_t ms = st;  // matching
         if (two) {
@@ -842,7 +902,11 @@ int vsfeel_bm3d_create_plane(const vsfeel_bm3d_args* args, const vsfeel_bm3d_vid
     ctx->acc_plane = (size_t)s.height * ctx->acc_pitch;
     if (const char* v = std::getenv("VSFEEL_FUSED_FILTER")) ctx->fused = v[0] == '1';
     if (const char* v = std::getenv("VSFEEL_OVERLAP_FILTER")) ctx->overlap = v[0] != '0';
-    if (const char* v = std::getenv("VSFEEL_MATCH_LANES")) ctx->match_lanes = std::atoi(v) == 16 ? 16 : 8;
+    if (const char* v = std::getenv("VSFEEL_MATCH_LANES")) {
+        ctx->match_lanes = std::atoi(v) == 16 ? 16 : 8;
+        ctx->autotune = false;  // an explicit choice is kept
+    }
+    if (const char* v = std::getenv("VSFEEL_AUTOTUNE")) ctx->autotune = ctx->autotune && v[0] != '0';
     DeviceGuard dg(device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();
@@ -1341,6 +1405,11 @@ int get_frame(vsfeel_bm3d* ctx, int n, bool with_ref,
             rc = stage(ctx->clampf(m - r), ctx->clampf(m + r));
             if (rc != VSFEEL_OK) return rc;
             float* slices = ctx->stack_slices(c);
+            if (!ctx->tuned)
+                ctx->ensure_tuned(ctx->stack_job(m, search, ctx->acc_pitch, 0, s.nframes - 1, nullptr,
+                                                 with_ref ? &input : nullptr, slices,
+                                                 ctx->match_xy.p, ctx->match_z.p),
+                                  st);
             VSF_CUDA(cudaMemsetAsync(slices, 0, sizeof(float) * (size_t)ctx->tw() * 2 * ctx->acc_plane,
                                      st));
             ctx->launch_stack(m, search, ctx->acc_pitch, 0, s.nframes - 1, st, nullptr, false,

@@ -501,7 +501,10 @@ int block_grid(const StackJob& job) { return (job.nbx * job.nby * 8 + kThreads -
 }  // namespace
 
 cudaError_t launch_match(const StackJob& job, cudaStream_t stream) {
-    const int shape = default_tile_shape(job, kTableOnly);
+    int shape = default_tile_shape(job, kTableOnly);
+    if (shape >= 0 && job.tile_shape_plus1 > 0 &&
+        tile_shape_fits(job, TileShape(job.tile_shape_plus1 - 1), kTableOnly))
+        shape = job.tile_shape_plus1 - 1;
     if (shape >= 0) return launch_match_tiles(job, TileShape(shape), kTableOnly, stream);
     if (job.radius < 3)
         bm3d_match_kernel<true><<<block_grid(job), kThreads, 0, stream>>>(job);
