@@ -110,6 +110,34 @@ def test_batch_classes_and_direct_read_fallback():
     assert batch.device_bytes > 0
 
 
+def test_batch_merged_and_per_stack_output_slots_agree(monkeypatch):
+    """Interior outputs of clips without the extractor keep one merged
+    accumulator pair (the default) instead of one per stack
+    (VSFEEL_MERGED_SLOTS=0): the same outputs within the bar, in less
+    device memory. Longer clips than CLIPS' so that most outputs are
+    interior."""
+    import torch
+
+    kws = [dict(sigma=5.0, block_step=4, bm_range=8, radius=2, ps_num=2, ps_range=3),
+           dict(sigma=6.0, block_step=4, bm_range=8, radius=1, ps_num=2, ps_range=3),
+           dict(sigma=4.0, block_step=4, bm_range=8, radius=1, ps_num=2, ps_range=3,
+                extractor_exp=2)]
+    src = [torch.from_numpy(make_clip(10, 64, 80, sigma=p["sigma"], shift=3, seed=40 + i)).cuda()
+           for i, p in enumerate(kws)]
+    outs, sizes = {}, {}
+    for merged in ("0", "1"):
+        monkeypatch.setenv("VSFEEL_MERGED_SLOTS", merged)
+        dst = [torch.full_like(s, float("nan")) for s in src]
+        batch = Batch(list(zip(src, dst, kws)), autotune=False)
+        _run(batch)
+        outs[merged], sizes[merged] = dst, batch.device_bytes
+    for i, (a, b) in enumerate(zip(outs["0"], outs["1"])):
+        assert bool(b.isfinite().all()), i
+        assert float((a - b).abs().max()) <= TOL, i
+    assert torch.equal(outs["0"][2], outs["1"][2])   # the extractor clip keeps its slices
+    assert sizes["1"] < sizes["0"]
+
+
 def test_batch_reruns_and_new_input():
     import torch
 

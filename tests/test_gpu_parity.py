@@ -181,6 +181,29 @@ def test_overlapped_and_serial_schedules_agree(monkeypatch):
         assert np.abs(a - b).max() <= tol, kw
 
 
+@pytest.mark.parametrize("kw,shape", [
+    (dict(sigma=3.0, block_step=4, bm_range=16, radius=2, ps_num=2, ps_range=7), (9, 136, 240)),
+    (dict(sigma=5.0, block_step=3, bm_range=8, radius=1, ps_num=3, ps_range=4), (6, 61, 93)),
+    (dict(sigma=6.0, block_step=4, bm_range=10, radius=3, ps_num=2, ps_range=5), (8, 72, 96)),
+])
+def test_merged_and_per_stack_output_slots_agree(kw, shape, monkeypatch, oracle_lib):
+    """Interior outputs accumulate all their stacks into one plane pair
+    (the default without the extractor) instead of one pair per stack
+    (VSFEEL_MERGED_SLOTS=0, the reference's slices): only float rounding
+    differs. Clip-end outputs (r of them at each end) keep per-stack slices
+    in both; both forms stay within the bar of the oracle."""
+    n, h, w = shape
+    frames = make_clip(n, h, w, sigma=kw["sigma"], shift=4, seed=63)
+    expected = oracle_lib.bm3d(frames, Params(**kw))
+    monkeypatch.setenv("VSFEEL_MERGED_SLOTS", "0")
+    sliced = _node(frames, **kw).output()
+    monkeypatch.setenv("VSFEEL_MERGED_SLOTS", "1")
+    merged = _node(frames, **kw).output()
+    assert float(np.abs(merged - sliced).max()) <= TYPICAL_TOL
+    for out in (merged, sliced):
+        assert float(np.abs(out.astype(np.float64) - expected).max()) <= TYPICAL_TOL
+
+
 def test_get_frame_matches_whole_clip():
     frames = make_clip(9, 72, 96, sigma=5.0, seed=3)
     node = _node(frames, sigma=5.0, block_step=4, bm_range=10, radius=2, ps_num=2, ps_range=4)

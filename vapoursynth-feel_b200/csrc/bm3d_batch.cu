@@ -147,8 +147,29 @@ struct Clip {
     size_t plane = 0;      // floats per accumulator plane
     size_t acc_off = 0;    // floats from the shared accumulator base (within its chunk)
     size_t table_off = 0;  // blocks from the shared match-table base (within its chunk)
+    // Output n's slot starts at plane pair pair0[n] (pair0[N]: all pairs).
+    // An interior output of a clip without the extractor has one merged
+    // (numerator, weight-origin) pair that all its stacks scatter into; the
+    // others keep one pair per contributing stack (the plain path's rule,
+    // vsfeel_bm3d::merged in bm3d_engine.cu).
+    std::vector<size_t> pair0;
+    bool merged_slots = false;
     int tw() const { return 2 * info.radius + 1; }
-    size_t acc_floats() const { return (size_t)info.num_frames * tw() * 2 * plane; }
+    bool merged(int n) const {
+        const int r = info.radius;
+        return merged_slots && n - r >= 0 && n + r <= info.num_frames - 1;
+    }
+    void plan_slots(bool allow_merge) {
+        merged_slots = allow_merge && info.extractor == 0.0f && info.radius > 0;
+        pair0.assign((size_t)info.num_frames + 1, 0);
+        for (int n = 0; n < info.num_frames; ++n)
+            pair0[n + 1] = pair0[n] + (merged(n) ? 1 : tw());
+    }
+    // First float of output n's slot pair j (j = 0 for a merged slot).
+    size_t pair_floats(int n, int j) const {
+        return (pair0[n] + (merged(n) ? 0 : j)) * 2 * plane;
+    }
+    size_t acc_floats() const { return pair0.back() * 2 * plane; }
 };
 
 using ClassKey = std::tuple<int, int, int, int, int>;  // radius, step, R, P, Q
@@ -250,8 +271,7 @@ struct vsfeel_bm3d_batch {
             job.slice_frame[z] = c.desc.src + (size_t)n * c.desc.src_frame_stride;
             job.slice_dst[z] = nullptr;
             if (silent || slice_reads(m, z, N, r) == 0) continue;
-            const int j = m - (n - r);
-            job.slice_dst[z] = acc_base + c.acc_off + ((size_t)n * tw + j) * 2 * c.plane;
+            job.slice_dst[z] = acc_base + c.acc_off + c.pair_floats(n, m - (n - r));
         }
         job.dst_plane = (int64_t)c.plane;
         job.pitch = (int)c.desc.src_row_stride;
@@ -481,10 +501,10 @@ void finish_class(vsfeel_bm3d_batch* b, Class& cls) {
                 NormalizeJob nj{};
                 for (int i = 0; i < tw; ++i) {
                     const int m = clampi(n - r + i, 0, N - 1);
-                    nj.num[i] = acc_base + c.acc_off + ((size_t)n * tw + (m - (n - r))) * 2 * c.plane;
+                    nj.num[i] = acc_base + c.acc_off + c.pair_floats(n, m - (n - r));
                 }
                 nj.den_offset = (int64_t)c.plane;
-                nj.tw = tw;
+                nj.tw = c.merged(n) ? 1 : tw;
                 nj.width = c.info.width;
                 nj.height = c.info.height;
                 nj.src_pitch = c.acc_pitch;
@@ -619,6 +639,8 @@ int vsfeel_bm3d_batch_create(const vsfeel_bm3d_batch_clip* clips, int nclips, in
     int rc = VSFEEL_OK;
     try {
         std::map<ClassKey, int> index;
+        bool merge_slots = true;  // VSFEEL_MERGED_SLOTS=0: one pair per stack everywhere
+        if (const char* v = std::getenv("VSFEEL_MERGED_SLOTS")) merge_slots = v[0] != '0';
         for (int i = 0; i < nclips; ++i) {
             const vsfeel_bm3d_batch_clip& d = clips[i];
             Clip c;
@@ -643,6 +665,7 @@ int vsfeel_bm3d_batch_create(const vsfeel_bm3d_batch_clip* clips, int nclips, in
                 throw Fail{VSFEEL_E_ARG, "clip " + std::to_string(i) + ": frame stride smaller than a plane"};
             c.acc_pitch = (d.width + 31) & ~31;
             c.plane = (size_t)d.height * c.acc_pitch;
+            c.plan_slots(merge_slots);
             b->clips.push_back(c);
             const ClassKey key{c.info.radius, c.info.block_step, c.info.bm_range, c.info.ps_num,
                                c.info.ps_range};

@@ -306,6 +306,18 @@ struct vsfeel_bm3d {
     // events; a pair replaces the default only when it is at least 2% faster.
     // Every pair gives the same match table.
     bool autotune = true;
+    // Merged output slots (VSFEEL_MERGED_SLOTS=0 turns them off): without the
+    // extractor, an interior output's 2r+1 contributing stacks scatter into
+    // one (numerator, weight-origin) plane pair of its ring slot instead of
+    // one pair each, and the normaliser reads that one pair. The reference
+    // sums its per-stack slices in FP64 after accumulating each in FP32; the
+    // merged FP32 sum differs from that by float rounding only (~1e-7 on the
+    // [0, 1] scale), like the reference's own atomic order from run to run.
+    // With the extractor the per-stack slices are kept, so that every slice
+    // sum stays exactly the reference's. An output within r of a clip end
+    // reads a clamped stack's slice more than once (the reference's
+    // weighting), so it keeps its per-stack slices too.
+    bool merge_slots = true;
     int tuned = 0;           // 0: not tuned yet; 1: tuned
     int tuned_shape_plus1 = 0;
     void ensure_tuned(const StackJob& sample_in, cudaStream_t st) {
@@ -527,6 +539,13 @@ struct vsfeel_bm3d {
     int clampf(int f) const { return clampi(f, 0, s.nframes - 1); }
 
     size_t ring_floats() const { return (size_t)tw() * tw() * 2 * acc_plane; }
+    // Whether output n's ring slot is one merged plane pair.
+    bool merged(int n) const {
+        return merge_slots && s.extractor == 0.0f && s.radius > 0 && n - s.radius >= 0 &&
+               n + s.radius <= s.nframes - 1;
+    }
+    // Plane pairs output n's ring slot uses.
+    int slot_pairs(int n) const { return merged(n) ? 1 : tw(); }
     float* slot_pair(int n, int j) {
         const int slot = n % tw();
         return ring.p + ((size_t)slot * tw() + j) * 2 * acc_plane;
@@ -578,8 +597,9 @@ struct vsfeel_bm3d {
             // slice z goes to the output that reads it: into that output's
             // ring slot, or (own_slices) into the stack's own slice z
             if (n >= out_lo && n <= out_hi && read_slice(n, m) == z)
-                job.slice_dst[z] = own_slices ? own_slices + (size_t)z * 2 * acc_plane
-                                              : slot_pair(n, m - (n - r));
+                job.slice_dst[z] = own_slices  ? own_slices + (size_t)z * 2 * acc_plane
+                                   : merged(n) ? slot_pair(n, 0)
+                                               : slot_pair(n, m - (n - r));
         }
         job.dst_plane = (int64_t)acc_plane;
         job.pitch = in_pitch;
@@ -655,6 +675,10 @@ struct vsfeel_bm3d {
         }
         job.den_offset = (int64_t)acc_plane;
         job.tw = tw();
+        if (!stack_slices_of && merged(n)) {
+            job.num[0] = slot_pair(n, 0);
+            job.tw = 1;
+        }
         job.width = s.width;
         job.height = s.height;
         job.src_pitch = acc_pitch;
@@ -760,7 +784,8 @@ struct vsfeel_bm3d {
             if (!two) {
                 for (int n = zeroed + 1; n <= want; ++n)
                     VSF_CUDA(cudaMemsetAsync(slot_pair(n, 0), 0,
-                                             sizeof(float) * (size_t)tw() * 2 * acc_plane, st));
+                                             sizeof(float) * (size_t)slot_pairs(n) * 2 * acc_plane,
+                                             st));
                 zeroed = std::max(zeroed, want);
                 if (before_stack) (*before_stack)(m, st);
                 launch_stack(m, frame_ptr, in_pitch, first, last, st, saved, false, input_ptr);
@@ -777,7 +802,8 @@ struct vsfeel_bm3d {
                 VSF_CUDA(cudaStreamWaitEvent(fs, ev_match[b], 0));
                 for (int n = zeroed + 1; n <= want; ++n)
                     VSF_CUDA(cudaMemsetAsync(slot_pair(n, 0), 0,
-                                             sizeof(float) * (size_t)tw() * 2 * acc_plane, fs));
+                                             sizeof(float) * (size_t)slot_pairs(n) * 2 * acc_plane,
+                                             fs));
                 zeroed = std::max(zeroed, want);
                 traced(VSFEEL_KERNEL_FILTER, fs, [&] { return launch_filter_beside_match(job, fs); });
                 VSF_CUDA(cudaEventRecord(ev_filter[b], fs));
@@ -907,6 +933,7 @@ int vsfeel_bm3d_create_plane(const vsfeel_bm3d_args* args, const vsfeel_bm3d_vid
         ctx->autotune = false;  // an explicit choice is kept
     }
     if (const char* v = std::getenv("VSFEEL_AUTOTUNE")) ctx->autotune = ctx->autotune && v[0] != '0';
+    if (const char* v = std::getenv("VSFEEL_MERGED_SLOTS")) ctx->merge_slots = v[0] != '0';
     DeviceGuard dg(device);
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
         cudaGetLastError();

@@ -35,6 +35,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstdio>
+#include <cstdlib>
 #include <mutex>
 
 namespace vsfeel {
@@ -203,8 +204,15 @@ int vsfeel_bm3d_process_device_noalloc(const vsfeel_bm3d_args* args,
     uint32_t* match_z = reinterpret_cast<uint32_t*>(base + off_z);
     float* ring = reinterpret_cast<float*>(base + off_ring);
     auto clampf = [&](int f) { return clampi(f, 0, N - 1); };
+    // An interior output of a clip without the extractor scatters all its
+    // stacks into one merged pair of its slot (the plain path's rule,
+    // vsfeel_bm3d::merged in bm3d_engine.cu); the others keep a pair per stack.
+    const char* merge_env = std::getenv("VSFEEL_MERGED_SLOTS");
+    const bool merge_slots = (merge_env == nullptr || merge_env[0] != '0') &&
+                             inf.extractor == 0.0f && r > 0;
+    auto merged = [&](int n) { return merge_slots && n - r >= 0 && n + r <= N - 1; };
     auto slot_pair = [&](int n, int j) {
-        return ring + ((size_t)(n % tw) * tw + j) * 2 * acc_plane;
+        return ring + ((size_t)(n % tw) * tw + (merged(n) ? 0 : j)) * 2 * acc_plane;
     };
     auto read_slice = [&](int n, int m) {
         for (int i = 0; i < tw; ++i)
@@ -226,8 +234,9 @@ int vsfeel_bm3d_process_device_noalloc(const vsfeel_bm3d_args* args,
         const int want = std::min(last, m + r);
         for (int n = zeroed + 1; n <= want; ++n)
             if ((rc = check(cudaMemsetAsync(slot_pair(n, 0), 0,
-                                            sizeof(float) * (size_t)tw * 2 * acc_plane, st))) !=
-                VSFEEL_OK)
+                                            sizeof(float) * (size_t)(merged(n) ? 1 : tw) * 2 *
+                                                acc_plane,
+                                            st))) != VSFEEL_OK)
                 return rc;
         zeroed = std::max(zeroed, want);
 
@@ -264,7 +273,7 @@ int vsfeel_bm3d_process_device_noalloc(const vsfeel_bm3d_args* args,
             NormalizeJob nj{};
             for (int i = 0; i < tw; ++i) nj.num[i] = slot_pair(n, clampf(n - r + i) - (n - r));
             nj.den_offset = (int64_t)acc_plane;
-            nj.tw = tw;
+            nj.tw = merged(n) ? 1 : tw;
             nj.width = W;
             nj.height = H;
             nj.src_pitch = acc_pitch;
