@@ -167,8 +167,8 @@ __device__ __forceinline__ void scatter_group(const StackJob& job, const uint32_
         float* pn = num + (size_t)my * dpitch + mx + sub;
 #pragma unroll
         for (int j = 0; j < 8; ++j)
-            atomicAdd(pn + (size_t)j * dpitch, __fsub_rn(__fmaf_rn(w, d[k * 8 + j], E), E));
-        if (sub == k) atomicAdd(num + job.dst_plane + (size_t)my * dpitch + mx, wv);
+            red_add_global(pn + (size_t)j * dpitch, __fsub_rn(__fmaf_rn(w, d[k * 8 + j], E), E));
+        if (sub == k) red_add_global(num + job.dst_plane + (size_t)my * dpitch + mx, wv);
     }
 }
 

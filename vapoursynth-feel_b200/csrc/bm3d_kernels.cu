@@ -490,7 +490,7 @@ __global__ void __launch_bounds__(128) bm3d_adjoint_kernel(const AdjointJob job)
         const int mx = (int)(mxy[k] & 0xffffu), my = (int)(mxy[k] >> 16);
         float* gi = job.grad_in + (size_t)f * job.gi_frame + (size_t)my * job.gi_pitch + mx + sub;
 #pragma unroll
-        for (int j = 0; j < 8; ++j) atomicAdd(gi + (size_t)j * job.gi_pitch, __fmul_rn(w, d[k * 8 + j]));
+        for (int j = 0; j < 8; ++j) red_add_global(gi + (size_t)j * job.gi_pitch, __fmul_rn(w, d[k * 8 + j]));
     }
 }
 

@@ -1086,14 +1086,14 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
             for (int e = threadIdx.x; e < acc.w * acc.h; e += blockDim.x) {
                 const float v = acc.num[e];
                 const int rr = e / acc.w, cc = e - rr * acc.w;
-                if (v != 0.0f) atomicAdd(num + (size_t)(acc.fy0 + rr) * dp + acc.fx0 + cc, v);
+                if (v != 0.0f) red_add_global(num + (size_t)(acc.fy0 + rr) * dp + acc.fx0 + cc, v);
             }
             const int ow = acc.w - 7;
             for (int e = threadIdx.x; e < ow * (acc.h - 7); e += blockDim.x) {
                 const float v = acc.org[e];
                 const int rr = e / ow, cc = e - rr * ow;
                 if (v != 0.0f)
-                    atomicAdd(num + job.dst_plane + (size_t)(acc.fy0 + rr) * dp + acc.fx0 + cc, v);
+                    red_add_global(num + job.dst_plane + (size_t)(acc.fy0 + rr) * dp + acc.fx0 + cc, v);
             }
         }
     }
