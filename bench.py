@@ -427,6 +427,10 @@ PROFILE_CASES = {
     # the batched form on a mixed handful of clips (one persistent launch per
     # class chunk)
     "batched_small": None,
+    # one 1080p radius-0 clip of 16 frames through the batched form (one
+    # chunk: one persistent matching launch, one filter launch over its 16
+    # stacks, one normalisation launch), 8x4 tiles
+    "batched_1920x1080x16_r0": None,
 }
 
 
@@ -448,6 +452,15 @@ def run_profile_case(torch, dev, name, steps, warmup):
                       device=dev.index or 0, autotune=False)
         run = batch.run
         px = sum(n * h * w for n, h, w, _ in spec)
+    elif name == "batched_1920x1080x16_r0":
+        from vsfeel.batch import Batch
+
+        p = dict(sigma=5.0, block_step=4, bm_range=16, radius=0, ps_num=2, ps_range=7)
+        x = make_clip_device(16, HEIGHT, WIDTH, p["sigma"], shift=4, seed=3100, device=dev)
+        out = torch.empty_like(x)
+        batch = Batch([(x, out, p)], device=dev.index or 0, autotune=False, tile_shape="8x4")
+        run = batch.run
+        px = x.numel()
     else:
         wl = PROFILE_CASES[name]
         x = make_clip_device(wl["frames"], wl["height"], wl["width"], sigma=wl["params"]["sigma"],
