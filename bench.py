@@ -352,6 +352,51 @@ def time_batched(torch, dev, steps, warmup):
             "max_abs_diff_vs_plain_first4": worst, "steps": steps, "warmup": warmup}
 
 
+def time_batched_sharded(torch, dev, rank, world, max_over_ranks, barrier, steps, warmup):
+    """The 64-clip workload across `world` ranks: whole clips, assigned
+    longest processing time first by the cost model (vsfeel.shard); every
+    rank builds and runs only its clips as one batch. Device time is the max
+    over ranks, and Mpx/s counts every clip's pixels once."""
+    import numpy as np
+
+    from vsfeel import shard as shard_mod
+    from vsfeel.batch import Batch
+    from vsfeel.synthetic import make_clip_device
+
+    spec = batched_clips(np.random.default_rng(3000))
+    costs = [shard_mod.clip_cost(*c) for c in spec]
+    plan = shard_mod.assign_clips(costs, world)
+    mine = plan[rank]
+    src = [make_clip_device(spec[i][0], spec[i][1], spec[i][2], spec[i][3]["sigma"], shift=4,
+                            seed=3000 + i, device=dev) for i in mine]
+    dst = [torch.empty_like(x) for x in src]
+    batch = Batch([(x, y, spec[i][3]) for x, y, i in zip(src, dst, mine)], device=dev.index,
+                  autotune=True) if mine else None
+    run = batch.run if batch else (lambda: None)
+    for _ in range(warmup):
+        run()
+    torch.cuda.synchronize()
+    barrier()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        run()
+    b.record()
+    torch.cuda.synchronize()
+    ms = max_over_ranks(a.elapsed_time(b) / steps)
+    if batch:
+        batch.finish()
+        batch.close()
+    px = sum(n * h * w for n, h, w, _ in spec)
+    loads = [sum(costs[i] for i in part) for part in plan]
+    return {"workload": "batched_64_clips_mixed_360p_to_2160p_x16_frames",
+            "batched_mpx_s": px / ms / 1e3, "batched_ms": ms,
+            "assignment": "whole clips, longest processing time first by the cost model",
+            "clips_per_rank": [len(part) for part in plan],
+            "predicted_ms_per_rank": [round(x, 2) for x in loads],
+            "steps": steps, "warmup": warmup}
+
+
 def time_all_planes(torch, dev, nfr, steps, warmup):
     """Per-plane denoising (the ``planes`` extension): a YUV420PS 1080p clip
     with all three planes denoised, the 960x540 chroma planes noisy like
@@ -731,6 +776,12 @@ def main() -> int:
                 "kernel_span_share": {k: round(ms / max(sum(x[0] for x in kt.values()), 1e-9), 4)
                                     for k, (ms, _) in kt.items()}}
 
+    # the batched form across ranks: every rank takes part (collectives)
+    batched_sharded = None
+    if world > 1 and not args.no_batch:
+        batched_sharded = time_batched_sharded(torch, dev, rank, world, max_over_ranks, barrier,
+                                               max(2, args.steps // 3), 3)
+
     if rank != 0:
         if world > 1:
             dist.destroy_process_group()
@@ -755,6 +806,8 @@ def main() -> int:
                            for name in GRAD_WORKLOADS]
     if world == 1 and not args.no_batch:
         line["batched"] = time_batched(torch, dev, max(2, args.steps // 3), 3)
+    if batched_sharded is not None:
+        line["batched"] = batched_sharded
     if world == 1 and not args.no_e2e:
         line["frame_requests"] = [time_frame_requests(luma, u, v, local_rank, 2, t)
                                   for t in (1, 4)]

@@ -136,3 +136,120 @@ def test_halo_recompute_fraction_of_the_sharded_bench(world, r):
 
     frac = sum(stacks(s) for s in plans) / (nfr * world) - 1.0
     assert abs(frac - 2 * r * (world - 1) / (nfr * world)) < 1e-12
+
+
+# ---------------------------------------------------------------------------
+# Many clips across ranks (the batched form): whole clips, longest processing
+# time first.
+
+@pytest.mark.parametrize("world", [1, 2, 3, 5, 8, 70])
+def test_assign_clips_gives_every_clip_to_one_rank_and_balances(world):
+    rng = np.random.default_rng(world)
+    costs = list(rng.uniform(0.5, 40.0, size=64))
+    plan = shard.assign_clips(costs, world)
+    assert len(plan) == world
+    flat = sorted(i for part in plan for i in part)
+    assert flat == list(range(64))
+    loads = [sum(costs[i] for i in part) for part in plan]
+    # greedy by falling cost: no rank ends more than one clip above the mean
+    assert max(loads) <= sum(costs) / world + max(costs) + 1e-9
+    assert plan == shard.assign_clips(costs, world)   # the same plan on every rank
+    for part in plan:
+        assert part == sorted(part)
+
+
+def test_assign_clips_takes_the_largest_first_and_breaks_ties_by_index():
+    assert shard.assign_clips([1.0, 5.0, 1.0, 3.0], 2) == [[1], [0, 2, 3]]
+    assert shard.assign_clips([2.0, 2.0, 2.0, 2.0], 2) == [[0, 2], [1, 3]]
+    assert shard.assign_clips([], 3) == [[], [], []]
+    with pytest.raises(ValueError):
+        shard.assign_clips([1.0], 0)
+    with pytest.raises(ValueError):
+        shard.assign_clips([-1.0], 1)
+
+
+def test_clip_cost_follows_the_work():
+    p2 = dict(sigma=3.0, block_step=4, bm_range=16, radius=2, ps_num=2, ps_range=7)
+    c1080 = shard.clip_cost(32, 1080, 1920, p2)
+    assert abs(c1080 - 32 * (1.81 + 0.175)) / c1080 < 0.01    # the measured 1080p r2 stack
+    assert shard.clip_cost(32, 2160, 3840, p2) > 3.9 * c1080
+    assert shard.clip_cost(32, 1080, 1920, dict(p2, radius=1)) < c1080
+    assert shard.clip_cost(32, 1080, 1920, dict(p2, block_step=8)) < c1080 / 3
+    # the exact search (radius >= 3) costs more per candidate
+    p4 = dict(p2, radius=4, ps_num=4)
+    cand4 = 33 ** 2 + 2 * 4 * 4 * 15 ** 2
+    assert shard.clip_cost(1, 1080, 1920, p4) > 128851 * cand4 * shard.MS_PER_SLIDING_CANDIDATE
+    assert shard.clip_cost(0, 1080, 1920, p2) == 0.0
+
+
+def test_assign_the_batched_workload():
+    """The 64-clip workload's plan: even at 2 and 4 ranks; at 8 the largest
+    clip (a 3840x2160 radius-2 clip) bounds the largest load."""
+    spec = []
+    rng = np.random.default_rng(3000)
+    sizes = [(640, 360)] * 16 + [(1280, 720)] * 24 + [(1920, 1080)] * 16 + [(3840, 2160)] * 8
+    for w, h in sizes:
+        spec.append((16, h, w, dict(sigma=float(rng.uniform(1.0, 10.0)),
+                                    block_step=int(rng.choice([4, 8])), bm_range=16,
+                                    radius=int(rng.choice([0, 1, 2])), ps_num=2, ps_range=7)))
+    costs = [shard.clip_cost(*s) for s in spec]
+    for world in (2, 4, 8):
+        loads = [sum(costs[i] for i in part) for part in shard.assign_clips(costs, world)]
+        assert max(loads) <= max(1.01 * sum(costs) / world, max(costs) + 1e-9), world
+
+
+SMALL_CLIPS = [
+    (4, 40, 48, dict(sigma=6.0, block_step=4, bm_range=5, radius=1, ps_num=2, ps_range=2)),
+    (3, 32, 40, dict(sigma=4.0, block_step=4, bm_range=4, radius=0)),
+    (5, 36, 44, dict(sigma=7.0, block_step=3, bm_range=4, radius=2, ps_num=2, ps_range=2)),
+    (3, 24, 32, dict(sigma=5.0, block_step=4, bm_range=4, radius=1, ps_num=1, ps_range=2,
+                     extractor_exp=2)),
+    (2, 48, 40, dict(sigma=3.0, block_step=8, bm_range=6, radius=0)),
+]
+
+
+def _small_clip(i):
+    n, h, w, p = SMALL_CLIPS[i]
+    return make_clip(n, h, w, sigma=p["sigma"], shift=2, seed=600 + i)
+
+
+def _clips_rank_main(rank, world, port, out_path):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    import datetime
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        costs = [shard.clip_cost(*c) for c in SMALL_CLIPS]
+        mine = shard.assign_clips(costs, world)[rank]
+        o = Oracle()
+        local = {i: o.bm3d(_small_clip(i), Params(**SMALL_CLIPS[i][3]), nthreads=2) for i in mine}
+        parts = [None] * world if rank == 0 else None
+        dist.gather_object(local, parts, dst=0)
+        if rank == 0:
+            merged = {}
+            for part in parts:
+                assert not set(part) & set(merged)   # no clip on two ranks
+                merged.update(part)
+            np.savez(out_path, **{str(i): merged[i] for i in sorted(merged)})
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_clips_across_two_gloo_ranks(tmp_path):
+    """Each rank denoises the clips the plan gives it (the oracle stands in
+    for the per-rank batch); gathered on rank 0, every clip is there once and
+    equals the single-process result."""
+    import torch.multiprocessing as mp
+
+    out = tmp_path / "clips.npz"
+    mp.start_processes(_clips_rank_main, args=(2, _free_port(), str(out)), nprocs=2, join=True,
+                       start_method="spawn")
+    got = np.load(out)
+    assert sorted(int(k) for k in got.files) == list(range(len(SMALL_CLIPS)))
+    o = Oracle()
+    for i, (_, _, _, p) in enumerate(SMALL_CLIPS):
+        assert np.array_equal(got[str(i)], o.bm3d(_small_clip(i), Params(**p), nthreads=2)), i
