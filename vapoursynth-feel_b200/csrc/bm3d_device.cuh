@@ -78,17 +78,25 @@ struct NormalizeBatch {
 struct AdjointJob {
     const unsigned char* saved;  // stack m's record at saved + m * stack_bytes
     int64_t stack_bytes, off_xy, off_z, off_mask;
-    const float* den;            // [N] planes of den_pitch floats per row
-    int64_t den_frame;
-    int den_pitch;
-    const float* grad_out;       // dL/d(output), frame f at grad_out + f * go_frame
-    int64_t go_frame;
-    int go_pitch;
+    const float* gs;             // scaled output gradient dL/d(output) / D of frame f
+                                 // in slot f % gs_slots, slots gs_frame floats apart
+    int64_t gs_frame;
+    int gs_pitch, gs_slots;
     float* grad_in;              // dL/d(input), accumulated (zero-filled by the caller)
     int64_t gi_frame;
     int gi_pitch;
     int nframes, radius, nblocks;
+    int first_stack, stack_count;  // this launch: stacks first_stack .. +stack_count-1
     int width, height;           // match positions are clamped to the frame
+};
+
+// One output frame's scaled gradient for the adjoint: gs = g / D per pixel
+// (the frozen denominator D of the forward's normalisation).
+struct GradScaleJob {
+    const float* go;   // dL/d(output) of the frame, go_pitch floats per row
+    const float* den;  // its frozen denominator, den_pitch floats per row
+    float* gs;         // out, gs_pitch floats per row
+    int go_pitch, den_pitch, gs_pitch, width, height;
 };
 
 // Tiled matcher (bm3d_match.cu): tile shapes in blocks, and what a tile
@@ -140,6 +148,7 @@ cudaError_t launch_filter_batch(const FilterBatch& work, int total_items, int gr
 inline int filter_items(int nblocks, int groups = 16) { return (nblocks + groups - 1) / groups; }
 cudaError_t launch_normalize(const NormalizeJob& job, cudaStream_t stream);
 cudaError_t launch_adjoint(const AdjointJob& job, cudaStream_t stream);
+cudaError_t launch_grad_scale(const GradScaleJob& job, cudaStream_t stream);
 cudaError_t launch_normalize_batch(const NormalizeBatch& work, int total_tiles, cudaStream_t stream);
 // The normaliser's tile: 2 rows (one warp each) of 120 pixels (30 lanes of
 // 4 pixels, the warp's other 2 lanes reading the 8-column halo on the left).

@@ -365,6 +365,7 @@ struct vsfeel_bm3d {
     }
 
     DevBuf<float> ring;       // (2r+1) slots x TW x {num, den} planes
+    DevBuf<float> gscale;     // the backward's scaled output gradients, a ring of frames
     DevBuf<uint32_t> match_xy;
     DevBuf<uint32_t> match_z;
     DevBuf<float> frames;     // staged input frames (host and frame paths)
@@ -969,6 +970,7 @@ void vsfeel_bm3d_free(vsfeel_bm3d* ctx) {
         ctx->ring.release();
         ctx->match_xy.release();
         ctx->match_z.release();
+        ctx->gscale.release();
         ctx->frames.release();
         ctx->outbuf.release();
         ctx->stackcache.release();
@@ -1596,28 +1598,63 @@ int vsfeel_bm3d_backward(vsfeel_bm3d* ctx, const void* saved, const float* grad_
                 VSF_CUDA(cudaMemset2DAsync(grad_in + (size_t)f * gi_frame_stride, pitch_bytes, 0,
                                            row_bytes, (size_t)s.height, st));
         }
+        // Stacks go in ranges of about eight waves of adjoint CTAs (three
+        // 128-thread CTAs per SM), in order. Before a range, the scaled
+        // gradients g / D of the frames it reads that no earlier range read
+        // are computed into a ring of count + 2r frame slots: the frames a
+        // range reads (its stacks -r .. +r) have distinct slots, and a slot
+        // it overwrites held a frame that no later stack reads.
+        const int r = s.radius;
+        int sms = 0;
+        VSF_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device));
+        // (the adjoint kernel: 128-thread CTAs of 16 groups, three per SM)
+        const int64_t target_groups = (int64_t)std::max(sms, 1) * 3 * 16 * 8;
+        const int per = (int)std::min<int64_t>(
+            s.nframes, std::max<int64_t>(1, (target_groups + ctx->nblocks - 1) / ctx->nblocks));
+        const int slots = std::min(s.nframes, per + 2 * r);
+        ctx->gscale.ensure((size_t)slots * ctx->frame_floats());
         AdjointJob job{};
         job.saved = base;
         job.stack_bytes = L.stack_bytes;
         job.off_xy = L.off_xy;
         job.off_z = L.off_z;
         job.off_mask = L.off_mask;
-        job.den = reinterpret_cast<const float*>(base + L.den_offset);
-        job.den_frame = (int64_t)ctx->frame_floats();
-        job.den_pitch = (int)L.den_pitch;
-        job.grad_out = grad_out;
-        job.go_frame = go_frame_stride;
-        job.go_pitch = (int)go_row_stride;
+        job.gs = ctx->gscale.p;
+        job.gs_frame = (int64_t)ctx->frame_floats();
+        job.gs_pitch = ctx->acc_pitch;
+        job.gs_slots = slots;
         job.grad_in = grad_in;
         job.gi_frame = gi_frame_stride;
         job.gi_pitch = (int)gi_row_stride;
         job.nframes = s.nframes;
-        job.radius = s.radius;
+        job.radius = r;
         job.nblocks = ctx->nblocks;
         job.width = s.width;
         job.height = s.height;
-        ctx->traced(VSFEEL_KERNEL_ADJOINT, st, [&] { return launch_adjoint(job, st); });
-        ctx->launches += 1;
+        const float* den = reinterpret_cast<const float*>(base + L.den_offset);
+        int scaled = -1;  // frames 0..scaled have their g / D in the ring
+        for (int m0 = 0; m0 < s.nframes; m0 += per) {
+            const int count = std::min(per, s.nframes - m0);
+            const int need = std::min(m0 + count - 1 + r, s.nframes - 1);
+            for (int f = scaled + 1; f <= need; ++f) {
+                GradScaleJob gj{};
+                gj.go = grad_out + (size_t)f * go_frame_stride;
+                gj.den = den + (size_t)f * ctx->frame_floats();
+                gj.gs = ctx->gscale.p + (size_t)(f % slots) * ctx->frame_floats();
+                gj.go_pitch = (int)go_row_stride;
+                gj.den_pitch = (int)L.den_pitch;
+                gj.gs_pitch = ctx->acc_pitch;
+                gj.width = s.width;
+                gj.height = s.height;
+                VSF_CUDA(launch_grad_scale(gj, st));
+                ctx->launches += 1;
+            }
+            scaled = std::max(scaled, need);
+            job.first_stack = m0;
+            job.stack_count = count;
+            ctx->traced(VSFEEL_KERNEL_ADJOINT, st, [&] { return launch_adjoint(job, st); });
+            ctx->launches += 1;
+        }
         ctx->mark_tail(st);
         return VSFEEL_OK;
     });
