@@ -263,7 +263,10 @@ VSFEEL_API int vsfeel_bm3d_forward_saved(vsfeel_bm3d* ctx, const float* src, int
                                          void* saved, void* stream);
 
 /* Writes dLoss/dInput into grad_in (overwritten) from dLoss/dOutput and the
- * saved state of a forward_saved call of the same context. */
+ * saved state of a forward_saved call of the same context. The context keeps
+ * a scratch ring of (stacks per adjoint launch + 2 * radius) frame planes for
+ * the scaled output gradient (dLoss/dOutput over the frozen denominator),
+ * allocated on the first call and freed with the context. */
 VSFEEL_API int vsfeel_bm3d_backward(vsfeel_bm3d* ctx, const void* saved, const float* grad_out,
                                     int64_t go_frame_stride, int64_t go_row_stride, float* grad_in,
                                     int64_t gi_frame_stride, int64_t gi_row_stride, void* stream);
