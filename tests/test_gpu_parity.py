@@ -2,9 +2,11 @@
 
 Bars: match tables identical to the oracle's (integer data, bit-exact);
 outputs within OUT_TOL of the reference on the [0, 1] scale. The only
-difference left is the order of float atomic adds into the aggregation
-slices, which the reference does not fix either
-(tests/test_bm3dv2.py:120-134 in the reference allow 1e-5 run to run).
+differences left are float rounding: the order of the atomic adds into the
+aggregation planes, which the reference does not fix either
+(tests/test_bm3dv2.py:120-134 in the reference allow 1e-5 run to run), and,
+without the extractor, one FP32 sum per interior output (merged slots) in
+place of the reference's FP64 sum of per-stack FP32 sums.
 """
 
 from __future__ import annotations
