@@ -154,6 +154,18 @@ def test_1080p_radius2_vs_oracle(oracle_lib):
     assert np.abs(out.astype(np.float64) - expected).max() <= TYPICAL_TOL
 
 
+def test_1080p_radius2_interior_output_vs_oracle(oracle_lib):
+    """The 1080p radius-2 workload on a 5-frame clip: output 2 reads five
+    distinct stacks, an interior output whose stacks scatter into one merged
+    accumulator pair (no extractor); against the oracle's per-stack slices
+    summed in FP64."""
+    p = Params(sigma=3.0, block_step=4, bm_range=16, radius=2, ps_num=2, ps_range=7)
+    frames = make_clip(5, 1080, 1920, sigma=3.0, shift=4, seed=2001)
+    expected = oracle_lib.bm3d(frames, p, out_first=2, out_count=1)
+    out = _node(frames, **p.as_dict()).output(first=2, count=1)
+    assert np.abs(out.astype(np.float64) - expected).max() <= TYPICAL_TOL
+
+
 def test_error_against_the_fp64_oracle(oracle_lib):
     """The CUDA path against the oracle's FP64 instantiation of the same
     algorithm: FP32 arithmetic moves a few threshold or ranking decisions,
