@@ -166,6 +166,18 @@ def test_1080p_radius2_interior_output_vs_oracle(oracle_lib):
     assert np.abs(out.astype(np.float64) - expected).max() <= TYPICAL_TOL
 
 
+def test_7680x4320_tables_and_output_vs_oracle(oracle_lib):
+    """The largest frames tested: 7680x4320 (8K UHD), radius 1, 3 frames;
+    the middle stack's table bit-exact and the middle output (an interior,
+    merged-slot output) within the bar."""
+    p = Params(sigma=4.0, block_step=4, bm_range=16, radius=1, ps_num=2, ps_range=7)
+    frames = make_clip(3, 4320, 7680, sigma=4.0, shift=4, seed=2002)
+    assert np.array_equal(_cuda_tables(frames, p, [1])[1], oracle_lib.matches(frames, p, 1))
+    expected = oracle_lib.bm3d(frames, p, out_first=1, out_count=1)
+    out = _node(frames, **p.as_dict()).output(first=1, count=1)
+    assert np.abs(out.astype(np.float64) - expected).max() <= TYPICAL_TOL
+
+
 def test_error_against_the_fp64_oracle(oracle_lib):
     """The CUDA path against the oracle's FP64 instantiation of the same
     algorithm: FP32 arithmetic moves a few threshold or ranking decisions,
