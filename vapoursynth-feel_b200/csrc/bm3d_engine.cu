@@ -292,9 +292,9 @@ struct vsfeel_bm3d {
     std::mutex lock;
     std::atomic<int64_t> launches{0};
     // Match and filter in one tiled launch (the match table stays on chip).
-    // Off by default: at the matcher's one CTA per SM the filter's atomics
-    // run slower than in the standalone filter kernel (3.18 vs 2.71 + 0.19 ms
-    // per 1080p stack on B200).
+    // Off by default: at the matcher's one CTA of 8 warps per SM the filter
+    // runs slower than the standalone filter kernel (2.41 against 1.81 + 0.16
+    // ms per 1080p radius-2 stack on B200).
     bool fused = false;
     // Lanes per reference block of the tiled sliding matcher (radius < 3):
     // 8 (256-thread CTAs) or 16 (512-thread CTAs, twice the warps per SM at
