@@ -669,10 +669,14 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
 // Scans windows[0..nwin) of this lane's block into its error table, then
 // selects the top-8 into gs->top. Rows are split into chunks of K
 // (warp-uniform); chunk c of the block goes to lane c % 8 in round c / 8.
-template <bool kExact, int kLanes>
+// after_scan() runs on every thread of the CTA once its warp has scanned,
+// before the selection, which reads the tables but not the staged region
+// (the caller stages the next phase's region there).
+template <bool kExact, int kLanes, class AfterScan>
 __device__ void search_windows(const Region& reg, const float* cur_s, const float c7[8],
                                const Window* wins, int nwin, float* E, GroupState* gs,
-                               unsigned gmask, int* status, bool probe) {
+                               unsigned gmask, int* status, bool probe,
+                               const AfterScan& after_scan) {
     static_assert(kLanes == 8 || (kLanes == 16 && !kExact), "16 lanes: sliding scan only");
     const int sub = threadIdx.x & (kLanes - 1);
     int total_rows = 0;
@@ -736,6 +740,7 @@ __device__ void search_windows(const Region& reg, const float* cur_s, const floa
         }
     }
     __syncwarp(gmask);
+    after_scan();
     // a window that was not scanned leaves stale values in the table; the
     // selection still ends (its pass limit) on in-range positions, and the
     // host reports the status word
@@ -761,10 +766,10 @@ __device__ __forceinline__ uint32_t key_xy(uint64_t key, const Window* wins, int
 // Stages frame rows [ry0, ry1] x columns [rx0, rx1] into smem, column-major
 // with column stride cs (odd, so the transposing stores of a warp hit
 // distinct banks). Global reads are coalesced along rows. The copies are
-// asynchronous (cp.async, 4 bytes each): a thread issues all of its copies
-// before waiting once, so the L2 latency of the region is paid about once
-// rather than once per dependent load and store. The caller synchronises
-// the CTA afterwards.
+// asynchronous (cp.async, 4 bytes each) and only issued here: a thread
+// issues all of its copies, and the caller waits once (cp.async.wait_all)
+// and synchronises the CTA before the region is read, so the L2 latency of
+// the region is paid about once, and can overlap other work meanwhile.
 __device__ void stage_region(float* smem, const float* __restrict__ frame, int pitch, int rx0,
                              int ry0, int rx1, int ry1, int cs) {
     const int w = rx1 - rx0 + 1;
@@ -778,7 +783,6 @@ __device__ void stage_region(float* smem, const float* __restrict__ frame, int p
                          : "memory");
         }
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // The same region row-major with row stride rs (the sliding scan).
@@ -795,7 +799,6 @@ __device__ void stage_region_rows(float* smem, const float* __restrict__ frame, 
                          : "memory");
         }
     }
-    asm volatile("cp.async.wait_all;" ::: "memory");
 }
 
 // windows a block holds at once: the spatial one, or ps_num temporal ones
@@ -937,7 +940,8 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         __syncwarp(gmask);
     }
 
-    auto stage = [&](const float* frame, int reach) {
+    // The staged region of a search phase: the tile +- reach, clamped.
+    auto region_of = [&](int reach) {
         Region s;
         const int rx0 = max(tile_x0 - reach, 0);
         const int rx1 = min(tile_x1 + reach, W - 8) + 7;
@@ -953,13 +957,36 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         s.rx1 = rx1;
         s.ry1 = ry1;
         s.smem = region;
-        __syncthreads();  // the previous phase has finished with the region
-        if (kExact)
-            stage_region(region, frame, pitch, rx0, ry0, rx1, ry1, s.cs);
-        else
-            stage_region_rows(region, frame, pitch, rx0, ry0, rx1, ry1, s.rs);
-        __syncthreads();
         return s;
+    };
+    // Issues the copies of a region (every thread; no wait).
+    auto issue = [&](const float* frame, const Region& s) {
+        if (kExact)
+            stage_region(region, frame, pitch, s.rx0, s.ry0, s.rx1, s.ry1, s.cs);
+        else
+            stage_region_rows(region, frame, pitch, s.rx0, s.ry0, s.rx1, s.ry1, s.rs);
+    };
+    auto wait_region = [] {
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
+    };
+    // The search phases: the spatial one (phase 0, frame r), then per
+    // direction dir = -1, +1 the temporal steps t = 1..r (frame r + dir t,
+    // reach R + t Q). Sliding scan: once every warp of the CTA has scanned
+    // phase p, the region is free, so the next phase's copies are issued
+    // then and land while the warps select and update their lists (the
+    // region does not depend on the predictors); the next scan waits for
+    // them (1.776 against 1.813 ms per 1080p radius-2 stack). The exact
+    // scan's selection is a short merge, so it stages each phase at its
+    // start (overlapping cost it 0.6%).
+    Region next{};
+    auto stage_next = [&](int dir, int t) {
+        return [&, dir, t] {
+            if (kExact || t == 0) return;  // staged at the phase's start / no next phase
+            __syncthreads();               // every warp has scanned: the region is free
+            next = region_of(R + t * Q);
+            issue(job.slice_frame[r + dir * t], next);
+        };
     };
 
     float ge = kFltMax;
@@ -967,11 +994,15 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
     int gz = 0;
 
     // spatial search (src/bm3d.comp:479-538)
+    __syncthreads();  // a previous tile of this CTA has finished with the region
+    Region s = region_of(R);
+    issue(fc, s);
+    wait_region();
     {
-        const Region s = stage(fc, R);
         if (sub == 0) win[0] = make_window(x, y, R, W, H, 0, 0);
         __syncwarp(gmask);
-        search_windows<kExact, kLanes>(s, cur_s, c7, win, 1, E, gs, gmask, job.status, probe);
+        search_windows<kExact, kLanes>(s, cur_s, c7, win, 1, E, gs, gmask, job.status, probe,
+                                       stage_next(-1, r >= 1 ? 1 : 0));
         const uint64_t k = gs->top[ent];
         const uint32_t xy = key_xy<kExact>(k, win, 0);
         // the global match list: lane `sub` holds entry sub & 7
@@ -989,7 +1020,13 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         __syncwarp(gmask);
         for (int t = 1; t <= r; ++t) {
             const int z = r + dir * t;
-            const Region s = stage(job.slice_frame[z], R + t * Q);
+            if (kExact) {
+                __syncthreads();  // the previous phase has finished with the region
+                next = region_of(R + t * Q);
+                issue(job.slice_frame[z], next);
+            }
+            wait_region();
+            s = next;
             if (sub == 0) {
                 int eoff = 0;
                 for (int i = 0; i < P; ++i) {
@@ -999,7 +1036,12 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
                 }
             }
             __syncwarp(gmask);
-            search_windows<kExact, kLanes>(s, cur_s, c7, win, P, E, gs, gmask, job.status, probe);
+            // the next phase: (dir, t + 1), or (+1, 1) after the last step of
+            // dir = -1, or none
+            const int ndir = t < r ? dir : 1;
+            const int nt = t < r ? t + 1 : (dir < 0 ? 1 : 0);
+            search_windows<kExact, kLanes>(s, cur_s, c7, win, P, E, gs, gmask, job.status, probe,
+                                           stage_next(ndir, nt));
             // the frame's first P matches enter the global list in order with
             // the reference's strict < (src/bm3d.comp:304-322): an entry goes
             // after the ones it does not beat; the group's lanes shift in
