@@ -785,11 +785,45 @@ __device__ void stage_region(float* smem, const float* __restrict__ frame, int p
     }
 }
 
-// The same region row-major with row stride rs (the sliding scan).
+// The same region row-major with row stride rs (the sliding scan). The
+// copies are issued right after the barrier that frees the region, on every
+// warp's path to its selection (about 9% of a 1080p radius-2 launch with
+// 4-byte copies), so when the source rows allow it (frame 8-byte aligned,
+// even pitch, even first column -- region_of starts the sliding scan's
+// region on an even column) each copy moves a column pair: 8-byte copies
+// over the flattened (row, pair) index, and an odd last column as a 4-byte
+// copy, so nothing past column rx1 is read. Otherwise 4-byte copies.
 __device__ void stage_region_rows(float* smem, const float* __restrict__ frame, int pitch, int rx0,
                                   int ry0, int rx1, int ry1, int rs) {
     const int w = rx1 - rx0 + 1;
     const int h = ry1 - ry0 + 1;
+    if (((reinterpret_cast<uintptr_t>(frame) & 7) | (pitch & 1) | (rx0 & 1)) == 0) {
+        const int npr = w >> 1, total = h * npr, nt = blockDim.x;
+        if (npr > 0) {
+            int row = threadIdx.x / npr, pr = threadIdx.x - row * npr;
+            const int dr = nt / npr, dp = nt - dr * npr;
+            for (int i = threadIdx.x; i < total; i += nt) {
+                const float* src = frame + (size_t)(ry0 + row) * pitch + rx0 + 2 * pr;
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(smem + row * rs + 2 * pr);
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src)
+                             : "memory");
+                pr += dp;
+                row += dr;
+                if (pr >= npr) {
+                    pr -= npr;
+                    ++row;
+                }
+            }
+        }
+        if (w & 1)
+            for (int yy = threadIdx.x; yy < h; yy += nt) {
+                const float* src = frame + (size_t)(ry0 + yy) * pitch + rx1;
+                const unsigned dst = (unsigned)__cvta_generic_to_shared(smem + yy * rs + (w - 1));
+                asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(dst), "l"(src)
+                             : "memory");
+            }
+        return;
+    }
     const int lane = threadIdx.x & 31;
     for (int yy = threadIdx.x >> 5; yy < h; yy += blockDim.x >> 5) {
         const float* __restrict__ row = frame + (size_t)(ry0 + yy) * pitch + rx0;
@@ -851,9 +885,10 @@ __host__ __device__ inline SmemPlan smem_plan(const StackJob& job, int mode) {
     const int w = tile_w + 2 * reach < job.width ? tile_w + 2 * reach : job.width;
     const int h = tile_h + 2 * reach < job.height ? tile_h + 2 * reach : job.height;
     // rows past the region that masked chunk rows read: at most kMaxK - 1;
-    // column-major for the exact scan, row-major for the sliding one
+    // column-major for the exact scan, row-major for the sliding one, whose
+    // region may start one column early (an even first column)
     const int cs = (h + kMaxK - 1) | 1;
-    p.region_floats = job.radius >= 3 ? cs * w : row_stride(w) * (h + kMaxK - 1);
+    p.region_floats = job.radius >= 3 ? cs * w : row_stride(w + 1) * (h + kMaxK - 1);
     // the exact scan (radius >= 3) selects without error tables; its table
     // area holds the block interleaved by column pairs (64 floats)
     const int tf = error_table_floats(job);
@@ -951,8 +986,11 @@ __device__ __forceinline__ void match_tile(const StackJob& job, int tile,
         // (a chunk starts at or above the window's last row and reads K + 6
         // rows below its start: at most kMaxK - 1 past the region)
         s.cs = (ry1 - ry0 + 1 + kMaxK - 1) | 1;
-        s.rs = row_stride(rx1 - rx0 + 1);
-        s.rx0 = rx0;
+        // the sliding scan's region starts on an even column, so that its
+        // rows are staged as column pairs (stage_region_rows)
+        const int rxs = kExact ? rx0 : (rx0 & ~1);
+        s.rs = row_stride(rx1 - rxs + 1);
+        s.rx0 = rxs;
         s.ry0 = ry0;
         s.rx1 = rx1;
         s.ry1 = ry1;
