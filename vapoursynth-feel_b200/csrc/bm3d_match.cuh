@@ -800,18 +800,23 @@ __device__ void stage_region_rows(float* smem, const float* __restrict__ frame, 
     if (((reinterpret_cast<uintptr_t>(frame) & 7) | (pitch & 1) | (rx0 & 1)) == 0) {
         const int npr = w >> 1, total = h * npr, nt = blockDim.x;
         if (npr > 0) {
-            int row = threadIdx.x / npr, pr = threadIdx.x - row * npr;
+            const int row = threadIdx.x / npr;
+            int pr = threadIdx.x - row * npr;
             const int dr = nt / npr, dp = nt - dr * npr;
+            const float* src = frame + (size_t)(ry0 + row) * pitch + rx0 + 2 * pr;
+            unsigned dst = (unsigned)__cvta_generic_to_shared(smem + row * rs + 2 * pr);
+            const ptrdiff_t src_step = (ptrdiff_t)dr * pitch + 2 * dp, src_wrap = pitch - 2 * npr;
+            const unsigned dst_step = 4u * (dr * rs + 2 * dp), dst_wrap = 4u * (rs - 2 * npr);
             for (int i = threadIdx.x; i < total; i += nt) {
-                const float* src = frame + (size_t)(ry0 + row) * pitch + rx0 + 2 * pr;
-                const unsigned dst = (unsigned)__cvta_generic_to_shared(smem + row * rs + 2 * pr);
                 asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(dst), "l"(src)
                              : "memory");
                 pr += dp;
-                row += dr;
+                src += src_step;
+                dst += dst_step;
                 if (pr >= npr) {
                     pr -= npr;
-                    ++row;
+                    src += src_wrap;
+                    dst += dst_wrap;
                 }
             }
         }
