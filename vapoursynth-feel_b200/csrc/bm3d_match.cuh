@@ -655,15 +655,35 @@ __device__ void select_top8(const float* E, const Window* wins, int nwin, float 
         tkey = t8;
         __syncwarp(gmask);
     }
-    if (sub < 8) gs->top[sub] = kKeyMax;
-    __syncwarp(gmask);
-    for (int j = sub; j < n; j += kLanes) {
-        const uint64_t kj = gs->buf[j];
-        int rank = 0;
-        for (int i = 0; i < n; ++i) rank += gs->buf[i] < kj ? 1 : 0;
-        if (rank < 8) gs->top[rank] = kj;
+    if (n <= 2 * kLanes) {
+        // up to two keys per lane, ranked by shuffles (the keys are distinct:
+        // every candidate of a phase has its own scan index)
+        const uint64_t k0 = sub < n ? gs->buf[sub] : kKeyMax;
+        const uint64_t k1 = sub + kLanes < n ? gs->buf[sub + kLanes] : kKeyMax;
+        int r0 = 0, r1 = 0;
+#pragma unroll
+        for (int j = 0; j < kLanes; ++j) {
+            const uint64_t o0 = __shfl_sync(gmask, k0, j, kLanes);
+            const uint64_t o1 = __shfl_sync(gmask, k1, j, kLanes);
+            r0 += (o0 < k0 ? 1 : 0) + (o1 < k0 ? 1 : 0);
+            r1 += (o0 < k1 ? 1 : 0) + (o1 < k1 ? 1 : 0);
+        }
+        if (sub < 8) gs->top[sub] = kKeyMax;
+        __syncwarp(gmask);
+        if (sub < n && r0 < 8) gs->top[r0] = k0;
+        if (sub + kLanes < n && r1 < 8) gs->top[r1] = k1;
+        __syncwarp(gmask);
+    } else {
+        if (sub < 8) gs->top[sub] = kKeyMax;
+        __syncwarp(gmask);
+        for (int j = sub; j < n; j += kLanes) {
+            const uint64_t kj = gs->buf[j];
+            int rank = 0;
+            for (int i = 0; i < n; ++i) rank += gs->buf[i] < kj ? 1 : 0;
+            if (rank < 8) gs->top[rank] = kj;
+        }
+        __syncwarp(gmask);
     }
-    __syncwarp(gmask);
 }
 
 // Scans windows[0..nwin) of this lane's block into its error table, then
