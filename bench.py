@@ -174,6 +174,16 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+TILE_NAMES = ("8x4", "16x2", "4x8", "8x2", "4x4")
+
+
+def matcher_config(info) -> dict:
+    """Tile shape (blocks) and lanes per block of the context's matcher."""
+    shape = info.match_tile_shape
+    return {"tile": TILE_NAMES[shape] if 0 <= shape < len(TILE_NAMES) else "direct-read",
+            "lanes_per_block": info.match_lanes, "autotuned": bool(info.autotuned)}
+
+
 def _device_id(torch, dev) -> str:
     try:
         u = str(torch.cuda.get_device_properties(dev).uuid)
@@ -768,6 +778,8 @@ def main() -> int:
                                 "fraction is far below it by the algorithm's 8 B/px",
                 "compute": compute,
                 "avg_launch_ms": avg_s * 1e3, "algorithmic_bytes_per_launch": alg_bytes,
+                # the matcher configuration the timed launches used
+                "match_kernel": matcher_config(node.info),
                 # summed event spans per kernel kind; filtering and normalisation run
                 # on a second stream beside the matching, so their spans overlap it
                 # and include waiting for SM space (the ncu launch list in profiles/

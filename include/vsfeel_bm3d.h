@@ -30,7 +30,7 @@
 extern "C" {
 #endif
 
-#define VSFEEL_BM3D_ABI_VERSION 2
+#define VSFEEL_BM3D_ABI_VERSION 3
 
 #if defined(__GNUC__)
 #define VSFEEL_API __attribute__((visibility("default")))
@@ -199,6 +199,12 @@ typedef struct vsfeel_bm3d_info {
     float extractor;  /* 2^extractor_exp, or 0 (src/bm3d.cpp:1188-1190)   */
     int blocks_x, blocks_y;
     int64_t device_bytes;  /* device memory held by the context           */
+    int match_tile_shape;  /* VSFEEL_TILE_* the matcher's table launches use
+                              (the autotuner's choice once it has run, the
+                              largest shape that fits before), or -1: the
+                              direct-read matcher                         */
+    int match_lanes;       /* lanes per block of the sliding matcher, 8 or 16 */
+    int autotuned;         /* 1 once the plain path's autotuner has run    */
 } vsfeel_bm3d_info;
 
 VSFEEL_API int vsfeel_bm3d_get_info(const vsfeel_bm3d* ctx, vsfeel_bm3d_info* info);

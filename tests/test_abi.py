@@ -161,6 +161,19 @@ def test_plane_params_plane_zero_equals_create():
     assert (inf.blocks_x, inf.blocks_y) == (13, 9)
 
 
+def test_plane_params_report_the_matcher_configuration():
+    """Before any autotuning the matcher uses the largest tile shape whose
+    shared-memory plan fits (8x4 blocks at the radius-2, step-4, range-16
+    settings) with 8 lanes per block; windows too large for every staged tile
+    go to the direct-read matcher (-1)."""
+    clip = vsfeel.clip_from_array(np.zeros((3, 270, 480), np.float32))
+    inf = vsfeel.plane_params(clip, 0, sigma=3.0, block_step=4, bm_range=16, radius=2,
+                              ps_num=2, ps_range=7)
+    assert (inf.match_tile_shape, inf.match_lanes, inf.autotuned) == (0, 8, 0)
+    big = vsfeel.plane_params(clip, 0, block_step=4, bm_range=60, radius=1)
+    assert big.match_tile_shape == -1
+
+
 @pytest.mark.parametrize("plane,fmt_yuv", [(1, False), (3, True), (-1, True)])
 def test_plane_outside_the_clip_is_rejected(plane, fmt_yuv):
     clip = _yuv420_clip() if fmt_yuv else vsfeel.clip_from_array(np.zeros((2, 16, 16), np.float32))

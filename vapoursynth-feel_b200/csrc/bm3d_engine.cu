@@ -855,6 +855,27 @@ namespace vsfeel {
 // Validates arguments as vsfeel_bm3d_create does and reports the effective
 // parameters, without touching the device (used by the allocation-free entry
 // point in bm3d_noalloc.cu).
+// The tile shape launch_match picks for table-mode matching of this
+// configuration: the autotuner's choice (1 + shape, 0: none) where it fits,
+// else the largest shape that fits; -1: the direct-read matcher.
+int table_tile_shape(const Settings& s, int nbx, int nby, int tuned_plus1) {
+    StackJob job{};
+    job.width = s.width;
+    job.height = s.height;
+    job.radius = s.radius;
+    job.step = s.step;
+    job.bm_range = s.bm_range;
+    job.ps_num = s.ps_num;
+    job.ps_range = s.ps_range;
+    job.nbx = nbx;
+    job.nby = nby;
+    int shape = default_tile_shape(job, kTableOnly);
+    if (shape >= 0 && tuned_plus1 > 0 &&
+        tile_shape_fits(job, TileShape(tuned_plus1 - 1), kTableOnly))
+        shape = tuned_plus1 - 1;
+    return shape;
+}
+
 int parse_to_info(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi,
                   vsfeel_bm3d_info* info, int plane) {
     Settings s;
@@ -875,6 +896,9 @@ int parse_to_info(const vsfeel_bm3d_args* args, const vsfeel_bm3d_video_info* vi
     info->extractor = s.extractor;
     info->blocks_x = block_count(s.width, s.step);
     info->blocks_y = block_count(s.height, s.step);
+    info->match_tile_shape = table_tile_shape(s, info->blocks_x, info->blocks_y, 0);
+    info->match_lanes = 8;
+    info->autotuned = 0;
     return VSFEEL_OK;
 }
 
@@ -1018,6 +1042,9 @@ int vsfeel_bm3d_get_info(const vsfeel_bm3d* ctx, vsfeel_bm3d_info* info) {
     info->blocks_y = ctx->nby;
     info->device_bytes = (int64_t)(ctx->ring.n + ctx->frames.n + ctx->outbuf.n + ctx->stackcache.n) * 4 +
                          (int64_t)(ctx->match_xy.n + ctx->match_z.n) * 4;
+    info->match_tile_shape = vsfeel::table_tile_shape(s, ctx->nbx, ctx->nby, ctx->tuned_shape_plus1);
+    info->match_lanes = ctx->match_lanes;
+    info->autotuned = ctx->tuned;
     return VSFEEL_OK;
 }
 

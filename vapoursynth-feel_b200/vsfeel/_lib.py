@@ -48,7 +48,7 @@ EXPORTS = (
     "vsfeel_bm3d_abi_version",
 )
 
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 OK = 0
 E_ARG = -1
@@ -109,6 +109,8 @@ class Info(ctypes.Structure):
         ("sigma", ctypes.c_float), ("threshold", ctypes.c_float), ("extractor", ctypes.c_float),
         ("blocks_x", ctypes.c_int), ("blocks_y", ctypes.c_int),
         ("device_bytes", ctypes.c_int64),
+        ("match_tile_shape", ctypes.c_int), ("match_lanes", ctypes.c_int),
+        ("autotuned", ctypes.c_int),
     ]
 
 
