@@ -204,7 +204,9 @@ typedef struct vsfeel_bm3d_info {
                               largest shape that fits before), or -1: the
                               direct-read matcher                         */
     int match_lanes;       /* lanes per block of the sliding matcher, 8 or 16 */
-    int autotuned;         /* 1 once the plain path's autotuner has run    */
+    int autotuned;         /* 1 once the plain path's autotuner has timed the
+                              shapes (0 while untuned, with VSFEEL_AUTOTUNE=0,
+                              radius >= 3 or the final pass)                */
 } vsfeel_bm3d_info;
 
 VSFEEL_API int vsfeel_bm3d_get_info(const vsfeel_bm3d* ctx, vsfeel_bm3d_info* info);

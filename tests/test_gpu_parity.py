@@ -448,10 +448,17 @@ def test_autotuned_and_default_contexts_agree(monkeypatch, oracle_lib):
     frames = make_clip(6, 256, 256, sigma=5.0, shift=3, seed=71)
     p = Params(**kw)
     monkeypatch.setenv("VSFEEL_AUTOTUNE", "0")
-    plain = _node(frames, **kw).output()
+    untuned = _node(frames, **kw)
+    plain = untuned.output()
+    # the context reports the configuration its matcher launches use
+    inf = untuned.info
+    assert (inf.match_tile_shape, inf.match_lanes, inf.autotuned) == (0, 8, 0)
     monkeypatch.setenv("VSFEEL_AUTOTUNE", "1")
     node = _node(frames, **kw)
     tuned = node.output()
+    inf = node.info
+    assert inf.autotuned == 1
+    assert 0 <= inf.match_tile_shape < 5 and inf.match_lanes in (8, 16)
     assert float(np.abs(tuned - plain).max()) <= TYPICAL_TOL
     assert float(np.abs(tuned.astype(np.float64) - oracle_lib.bm3d(frames, p)).max()) <= TYPICAL_TOL
     for m in (0, 3, 5):

@@ -318,7 +318,8 @@ struct vsfeel_bm3d {
     // reads a clamped stack's slice more than once (the reference's
     // weighting), so it keeps its per-stack slices too.
     bool merge_slots = true;
-    int tuned = 0;           // 0: not tuned yet; 1: tuned
+    int tuned = 0;           // 0: not tuned yet; 1: tuned (or tuning skipped)
+    int tuner_ran = 0;       // 1: the autotuner timed the shapes
     int tuned_shape_plus1 = 0;
     void ensure_tuned(const StackJob& sample_in, cudaStream_t st) {
         if (tuned || !autotune || sample_in.radius >= 3 || sample_in.wiener) {
@@ -328,6 +329,7 @@ struct vsfeel_bm3d {
         tuned = 1;
         const int def = default_tile_shape(sample_in, kTableOnly);
         if (def < 0) return;
+        tuner_ran = 1;
         StackJob sample = sample_in;
         for (int z = 0; z < kMaxTW; ++z) sample.slice_dst[z] = nullptr;  // table only
         cudaEvent_t e0 = next_event(), e1 = next_event();
@@ -1044,7 +1046,7 @@ int vsfeel_bm3d_get_info(const vsfeel_bm3d* ctx, vsfeel_bm3d_info* info) {
                          (int64_t)(ctx->match_xy.n + ctx->match_z.n) * 4;
     info->match_tile_shape = vsfeel::table_tile_shape(s, ctx->nbx, ctx->nby, ctx->tuned_shape_plus1);
     info->match_lanes = ctx->match_lanes;
-    info->autotuned = ctx->tuned;
+    info->autotuned = ctx->tuner_ran;
     return VSFEEL_OK;
 }
 
