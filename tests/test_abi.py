@@ -210,3 +210,37 @@ def test_all_planes_reach_the_device_check_without_a_gpu():
         pytest.skip("a GPU is present")
     with pytest.raises(vsfeel.Error, match="no CUDA device"):
         vsfeel.BM3Dv2(_yuv420_clip(), planes=[0, 1, 2], sigma=[3.0, 5.0], block_step=[4, 2])
+
+
+def test_ctypes_structs_match_the_header_layout(tmp_path):
+    """Every struct the ctypes stub mirrors has the header's size and member
+    offsets (gcc compiles the header and prints them), so a member added on
+    one side only fails here instead of corrupting a call."""
+    import ctypes
+    import shutil
+    import subprocess
+
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc is not installed")
+    pairs = [("vsfeel_bm3d_video_info", _lib.VideoInfo), ("vsfeel_bm3d_args", _lib.Args),
+             ("vsfeel_bm3d_info", _lib.Info), ("vsfeel_bm3d_saved_info", _lib.SavedInfo),
+             ("vsfeel_bm3d_batch_clip", _lib.BatchClip),
+             ("vsfeel_bm3d_batch_class_info", _lib.BatchClassInfo)]
+    src = ["#include <stdio.h>", "#include <stddef.h>", '#include "vsfeel_bm3d.h"',
+           "int main(void) {"]
+    want = []
+    for cname, cls in pairs:
+        src.append(f'printf("%zu\\n", sizeof({cname}));')
+        want.append(ctypes.sizeof(cls))
+        for name, *_ in cls._fields_:
+            src.append(f'printf("%zu\\n", offsetof({cname}, {name}));')
+            want.append(getattr(cls, name).offset)
+    src.append("return 0; }")
+    (tmp_path / "layout.c").write_text("\n".join(src))
+    include = ROOT / "include"
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", str(include), str(tmp_path / "layout.c"), "-o", str(exe)],
+                   check=True, capture_output=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    assert got == want
