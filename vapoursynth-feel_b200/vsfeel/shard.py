@@ -94,12 +94,12 @@ def gather(local: np.ndarray, shards: list[Shard], rank: int, group=None, dst: i
     return np.concatenate([p for p in parts if p is not None and len(p)], axis=0)
 
 
-# Measured on one B200 (CUDA events, kernels serialised): the sliding
-# matcher (radius < 3) at 1.776 ms per 1080p radius-2 stack of 368.5 M
-# candidates; the exact matcher (radius >= 3) at 46.6 ms per 3840x2160
+# Measured on one B200 (CUDA events): the sliding matcher (radius < 3) at
+# 1.609 ms per 1080p radius-2 stack of 368.5 M candidates (the autotuner's
+# tile); the exact matcher (radius >= 3) at 46.6 ms per 3840x2160
 # radius-4 stack of 4.28 G candidates; the filter and normalisation at
 # 0.175 ms per 128,851 blocks.
-MS_PER_SLIDING_CANDIDATE = 1.776 / 368.5e6
+MS_PER_SLIDING_CANDIDATE = 1.609 / 368.5e6
 MS_PER_EXACT_CANDIDATE = 46.6 / 4.28e9
 MS_PER_BLOCK = 0.175 / 128851
 
